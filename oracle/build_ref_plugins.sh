@@ -1,0 +1,17 @@
+#!/bin/sh
+# Compiles the reference's C example plugins (hkbelagali/propaq,
+# examples/plugins/c/{noise,truncation}/*.c) from the reference tree into
+# oracle/_ref/, with the same flags the reference's notebooks use
+# (examples/plugins/notebooks/02_rust_plugins.ipynb).  These plugins are test
+# fixtures for the plugin ABI; nothing in the product links them.
+set -e
+REF=${PROPAQ_REFERENCE:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+[ -d "$REF/examples/plugins/c" ] || { echo "reference tree not found at $REF" >&2; exit 1; }
+mkdir -p "$OUT"
+for src in "$REF"/examples/plugins/c/noise/*.c "$REF"/examples/plugins/c/truncation/*.c; do
+  name=$(basename "$src" .c)
+  gcc -shared -fPIC -O2 -o "$OUT/$name.so" "$src" -lm
+done
+ls "$OUT"
