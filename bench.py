@@ -1,0 +1,359 @@
+"""Benchmark of the propagation hot path (one JSON line on rank 0).
+
+A step is one full Heisenberg propagation of the workload plus its expectation
+value.  The default workload is the large noisy Pauli configuration: a 10x10
+open-lattice kicked Ising circuit (20 steps of RZZ(-pi/2) on the 4 edge colour
+classes + RX(0.6) on all qubits), observable Z at the centre, depolarising
+p = 1e-3 per qubit per layer as (1-p)^weight damping, weight cutoff 10,
+coefficient cutoff 1e-5, FP64 coefficients.
+
+    value  = sum over gates of the live terms after the gate, per second of
+             device time (CUDA events on the engine's stream, inputs resident)
+    e2e    = the same metric through PauliPropagator.expectation_value with
+             host inputs, host<->device copies inside the timed region
+    roofline: the gate kernel's algorithmic bytes (8W N + 16 A + (8+8W) A +
+             (8W+16) E per gate, N live rows, A anticommuting rows, E children)
+             over its event-timed duration, against the measured HBM copy
+             bandwidth.
+
+`--impl reference` times the CPU restatement of the reference engine (the
+oracle) on the host cores instead.  With torchrun (N > 1) every rank runs an
+independent replica of the workload (the path does not shard).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "majorana", "tfim"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(name):
+    from propaq_b200 import workloads
+
+    if name == "kicked_ising":
+        wl = workloads.kicked_ising()
+        desc = ("kicked Ising 10x10 open lattice, 20 steps, RZZ(-pi/2) x 180 edges + RX(0.6) x 100 per step, "
+                "Z(centre), p=1e-3 depolarising as (1-p)^w, w<=10, |c|>=1e-5")
+    elif name == "majorana":
+        wl = workloads.majorana_givens()
+        desc = ("Majorana 32 sites / 64 modes, 4 reps of brick-wall Givens + number-number phases |p-q|<=3, "
+                "sum_p c_p g2p g2p+1, half filling, JW w<=8, |c|>=1e-6")
+    else:
+        wl = workloads.tfim_chain()
+        desc = "TFIM chain 20 qubits, 10 Trotter layers, Z10, w<=8, |c|>=1e-4"
+    return wl, desc
+
+
+def measured_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.dev), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def gate_bytes(W, rows, anti, children):
+    return 8 * W * rows + 16 * anti + (8 + 8 * W) * anti + (8 * W + 16) * children
+
+
+def run_cpu_baseline(problem_builder, seconds, cores):
+    """The oracle (CPU restatement of the reference engine) over whole runs of
+    the workload, as many as fit in `seconds` (at least one)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from harness import run_oracle
+    from oracle_client import Oracle
+
+    o = Oracle.load()
+    p = problem_builder()
+    runs, terms, t0 = 0, 0, time.perf_counter()
+    while True:
+        r = run_oracle(o, p, n_partitions=cores, want_terms=False)
+        runs += 1
+        terms += int(r.n_terms.sum())
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return terms / el, runs, el, r
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    wl, desc = make_workload(args.workload)
+    cores = os.cpu_count() or 1
+    W = 1
+    while 32 * W < wl.n_units:
+        W *= 2
+
+    def builder():
+        sys.path.insert(0, str(ROOT / "tests"))
+        from harness import from_workload
+
+        return from_workload(wl)
+
+    base_line = {"metric": "terms/s", "unit": "terms/s", "n_gpus": args.gpus, "steps": args.steps,
+                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                 "dtype": "f64", "data": "synthetic (seeded; no dataset)",
+                 "config": {"workload": desc, "name": wl.name, "n_units": wl.n_units, "key_words": W,
+                            "gates": len(wl.circuit.rotations), "layers": len(wl.circuit.layers),
+                            "parallelism": f"replicas x{world}", "l2": "flushed between steps"}}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps_t, terms_total = [], 0
+        sys.path.insert(0, str(ROOT / "tests"))
+        from harness import run_oracle
+        from oracle_client import Oracle
+
+        o = Oracle.load()
+        p = builder()
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            r = run_oracle(o, p, n_partitions=cores, want_terms=False)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                steps_t.append(dt)
+                terms_total += int(r.n_terms.sum())
+        total = sum(steps_t)
+        v = terms_total / total
+        line = dict(base_line, impl="reference", value=v, ms_per_step=1e3 * total / len(steps_t),
+                    cpu_baseline={"value": v, "unit": "terms/s", "cores": cores, "kind": "port",
+                                  "sample": f"whole workload per step, oracle with {cores} partitions/threads"},
+                    e2e={"value": v, "unit": "terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                    expectation_value=r.expectation)
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    from propaq_b200 import MajoranaPropagator, PauliPropagator, _native
+
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    engine = _native.engine(local)
+    prob = builder()
+    # A 512 MB write between steps evicts the 126 MB L2.
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    cfg = _native.RunConfig()
+    cfg.basis_kind = prob.basis
+    cfg.n_units = prob.n_units
+    cfg.max_weight = -1 if prob.max_weight is None else prob.max_weight
+    cfg.has_min_coeff = 0 if prob.min_coeff is None else 1
+    cfg.min_coeff = 0.0 if prob.min_coeff is None else prob.min_coeff
+    cfg.min_terms = -1
+    table = None
+    if prob.noise_table is not None:
+        table = np.ascontiguousarray(prob.noise_table, dtype=np.float64)
+        cfg.noise_kind, cfg.noise_tables, cfg.noise_table_len = _native.PQ_NOISE_TABLE, table.ctypes.data, len(table)
+    cfg.want_terms = 0
+    cfg.profile = 1
+
+    def device_step():
+        return engine.run(cfg, prob.obs_keys, prob.obs_coeffs, prob.gate_keys, prob.angles, prob.offsets, prob.diag)
+
+    prop_cls = PauliPropagator if wl.basis == 0 else MajoranaPropagator
+    prop = prop_cls(noise=wl.noise(), truncation=wl.truncation(), device=local)
+
+    def api_step():
+        return prop.expectation_value(wl.observable, wl.circuit, initial_state=wl.initial_state)
+
+    def settle():
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier(world)
+
+    for _ in range(args.warmup):
+        settle()
+        device_step()
+        settle()
+        api_step()
+
+    dev_ms = gate_ms = noise_ms = 0.0
+    terms = launches = gate_ops = 0
+    galg = nalg = 0
+    e2e_s = 0.0
+    e2e_terms = 0
+    peak = 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            settle()
+            res, nt = device_step()
+            torch.cuda.synchronize()
+            dev_ms += res.device_ms
+            terms += int(nt.sum())
+            launches += int(res.gpu_launches)
+            gate_ms += res.gate_ms
+            noise_ms += res.noise_ms
+            gate_ops += int(res.gate_ops)
+            peak = max(peak, int(res.peak_terms))
+            galg += gate_bytes(W, res.sum_rows_gate, res.sum_anti, res.sum_children)
+            nalg += (8 * W + 16) * (res.sum_rows_noise + res.sum_kept)
+        for _ in range(args.steps):
+            settle()
+            t0 = time.perf_counter()
+            r = api_step()
+            torch.cuda.synchronize()
+            e2e_s += time.perf_counter() - t0
+            e2e_terms += sum(r.n_terms)
+    clocks = clk.summary()
+    dev_s = max_over_ranks(world, dev_ms / 1e3)
+    e2e_s = max_over_ranks(world, e2e_s)
+    value = world * terms / dev_s
+    e2e_value = world * e2e_terms / e2e_s
+    # host <-> device bytes per step of pq_run: observable, gates, offsets,
+    # state and noise table in; per-gate counts, per-op counters and the
+    # expectation partials out.
+    n_ops = len(prob.angles) + len(prob.offsets) - 1
+    h2d = (prob.obs_keys.nbytes + prob.obs_coeffs.nbytes + prob.gate_keys.nbytes + prob.angles.nbytes
+           + prob.offsets.nbytes + (0 if prob.diag is None else prob.diag.nbytes)
+           + (0 if table is None else table.nbytes))
+    d2h = 8 * len(prob.angles) + 16 * n_ops + 32 * 4 * 148
+    peak_gbs, peak_kind = measured_peaks()
+    achieved = galg / (gate_ms / 1e3) / 1e9 if gate_ms > 0 else None
+    traffic = None
+    tf = ROOT / "profiles" / f"gate_kernel_traffic_{wl.name}.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
+    line = dict(base_line, value=value, ms_per_step=1e3 * dev_s / args.steps,
+                e2e={"value": e2e_value, "unit": "terms/s", "h2d_bytes_per_step": int(h2d),
+                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s / args.steps},
+                gpu_launches=launches,
+                roofline={"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+                          "frac": None if achieved is None else achieved / peak_gbs, "traffic": traffic,
+                          "kernel": "gate_kernel", "peak_source": f"{peak_kind} hbm_gbs",
+                          "algorithmic_bytes_per_launch": galg / max(1, gate_ops),
+                          "ms_per_launch": gate_ms / max(1, gate_ops),
+                          "share_of_device_time": gate_ms / dev_ms if dev_ms else None,
+                          "noise_kernel_gbs": nalg / (noise_ms / 1e3) / 1e9 if noise_ms > 0 else None},
+                clocks=clocks, peak_terms=peak, expectation_value=r.expectation_value)
+    line["config"]["parallelism"] = f"replicas x{world}"
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, runs, el, _ = run_cpu_baseline(builder, args.cpu_seconds, cores)
+        line["cpu_baseline"] = {"value": v, "unit": "terms/s", "cores": cores, "kind": "port",
+                                "sample": f"{runs} whole run(s) of the workload in {el:.1f} s, oracle with "
+                                          f"{cores} partitions/threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+/*
+ * propaq_cuda.h -- C ABI of the B200 propagation engine (libpropaq_cuda.so).
+ *
+ * The engine applies a circuit of Pauli/Majorana rotations to a sparse sum of
+ * packed bitstrings with FP64 coefficients in the Heisenberg picture: it
+ * branches anticommuting terms, merges duplicates, truncates by weight and
+ * coefficient, damps by noise, and reduces the expectation value against a
+ * computational-basis state.  Everything between the first and last call of
+ * pq_run happens on one GPU.
+ *
+ * Every entry point below replaces one interface of the reference
+ * (hkbelagali/propaq); each comment names the file:line it stands in for.
+ *
+ * Conventions
+ *   - Keys are `n_words` u64 words per term, two bits per unit, interleaved:
+ *     Pauli qubit q uses bit 2q (x) and 2q+1 (z); Majorana mode m uses bit m,
+ *     so site k owns modes 2k and 2k+1 (crates/pauli/src/algebra.rs:242-257,
+ *     crates/majorana/src/algebra.rs:218-233).  n_words comes from
+ *     pq_words_for_units (crates/pauli/src/engine.rs:289-301).
+ *   - All functions return PQ_OK (0) or a PQ_ERR_* code; no exception crosses
+ *     the ABI.  pq_engine_last_error gives the message of the last failure.
+ *   - The engine owns all device memory; the caller owns every host array.
+ *     One engine = one CUDA stream; an engine is not re-entrant, distinct
+ *     engines may be used from distinct threads.
+ */
+#ifndef PROPAQ_CUDA_H
+#define PROPAQ_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PQ_ABI_VERSION 1u
+
+/* Status codes.  The Python layer maps them to the reference's exception
+ * types: INVALID -> ValueError (crates/pauli/src/propagator.rs:256-260),
+ * CEILING -> RuntimeError (crates/core/src/storage/operator_index.rs:116-127),
+ * PLUGIN_LOAD -> OSError and PLUGIN -> ValueError
+ * (crates/core/src/policy/native_noise.rs:217-260). */
+enum {
+  PQ_OK = 0,
+  PQ_ERR_INVALID = 1,        /* bad argument, width beyond 2048 units, odd modes */
+  PQ_ERR_CUDA = 2,           /* CUDA runtime failure or no usable device          */
+  PQ_ERR_OOM = 3,            /* device allocation failed                          */
+  PQ_ERR_CEILING = 4,        /* live terms would exceed the engine's row ceiling  */
+  PQ_ERR_PLUGIN_LOAD = 5,    /* dlopen failed                                     */
+  PQ_ERR_PLUGIN = 6,         /* plugin symbol / ABI / dependency validation       */
+  PQ_ERR_DEVICE_TIMEOUT = 7, /* a bounded device-side wait expired                */
+  PQ_ERR_UNSUPPORTED = 8     /* a configuration this build does not run           */
+};
+
+enum { PQ_BASIS_PAULI = 0, PQ_BASIS_MAJORANA = 1 };
+
+/* How noise reaches the engine (crates/core/src/engine/noise_resolver.rs:28-37). */
+enum {
+  PQ_NOISE_NONE = 0,
+  PQ_NOISE_TABLE = 1,   /* one factor per weight, table_len entries              */
+  PQ_NOISE_LAYERED = 2, /* n_layers tables of table_len entries, one per layer   */
+  PQ_NOISE_PLUGIN = 3   /* a loaded plugin; the engine resolves it by `depends`  */
+};
+
+typedef struct pq_engine pq_engine;
+typedef struct pq_plugin pq_plugin;
+
+/* One run's truncation and noise, the flattened form of
+ * crates/core/src/policy/truncators.rs:188-213 (ResolvedConfig) plus the
+ * resolved noise model. */
+typedef struct pq_run_config {
+  uint32_t basis_kind;       /* PQ_BASIS_*                                      */
+  uint32_t n_units;          /* qubits (Pauli) or sites = modes / 2 (Majorana)  */
+  int64_t max_weight;        /* WeightTruncator; < 0 = none                     */
+  uint32_t has_min_coeff;    /* CoefficientTruncator present                    */
+  double min_coeff;
+  int64_t min_terms;         /* TermBudget floor; < 0 = none                    */
+  const pq_plugin* truncator;/* NativeTruncator, or NULL                        */
+  uint32_t noise_kind;       /* PQ_NOISE_*                                      */
+  const double* noise_tables;/* TABLE / LAYERED factors                         */
+  size_t noise_table_len;    /* entries per table (normally n_units + 1)       */
+  const pq_plugin* noise_plugin; /* PLUGIN kind                                 */
+  uint32_t want_terms;       /* keep the final terms for pq_result_terms        */
+  uint32_t profile;          /* time every op with CUDA events (pq_result *_ms) */
+} pq_run_config;
+
+/* crates/core/src/interface/results.rs:8-51 (PropagationResult), plus the
+ * engine's own counters. */
+typedef struct pq_result {
+  double expectation_value;   /* 0 when no diag_state was given               */
+  uint64_t terms_below_cutoff;/* live terms with |c| < min_coeff at the end   */
+  uint64_t sparse_key_bytes;  /* device bytes holding keys and the hash table */
+  uint64_t n_final;           /* live terms at the end                        */
+  uint64_t n_layers_run, n_gates_run;
+  uint64_t gpu_launches;      /* kernels this run launched                    */
+  uint64_t peak_terms;        /* largest live count seen                      */
+  double device_ms;           /* device time of the gate loop (CUDA events)   */
+  /* Per-kind totals; the *_ms fields are filled only with cfg->profile. */
+  double gate_ms, noise_ms, phase_ms;
+  uint64_t gate_ops, noise_ops, phase_ops;
+  uint64_t sum_rows_gate;     /* sum over gate ops of the live rows they scan  */
+  uint64_t sum_anti;          /* ... of the rows anticommuting with the gate   */
+  uint64_t sum_children;      /* ... of the children they append               */
+  uint64_t sum_rows_noise;    /* sum over noise ops of the rows they scan      */
+  uint64_t sum_kept;          /* ... of the rows a reclaim keeps               */
+} pq_result;
+
+/* Key width for a register: 1,2,4,...,64 words for up to 32,64,...,2048
+ * qubits (Pauli) or sites (Majorana); 0 if beyond the 2048-unit maximum.
+ * Replaces runner_for, crates/pauli/src/engine.rs:289-301. */
+uint32_t pq_words_for_units(uint32_t n_units);
+
+/* Creates an engine on CUDA device `device`.  Replaces the rayon pool of
+ * crates/core/src/engine/run_config.rs:13-55. */
+int pq_engine_create(pq_engine** out, int device);
+void pq_engine_destroy(pq_engine* engine);
+const char* pq_engine_last_error(const pq_engine* engine);
+
+/* Runs one propagation; replaces engine::run / run_at_width
+ * (crates/pauli/src/engine.rs:74-238, :305-357; crates/majorana/src/engine.rs).
+ *
+ *   obs_words   n_obs * n_words   observable keys (duplicates are added)
+ *   obs_coeffs  n_obs             observable coefficients
+ *   gate_words  n_gates * n_words generators in HEISENBERG order: circuit
+ *                                 layers reversed and the gates of each layer
+ *                                 reversed (extract_layers, engine.rs:44-70)
+ *   gate_angles n_gates           rotation angles (U = exp(-i angle G / 2))
+ *   layer_offsets n_layers + 1    layer l holds gates [off[l], off[l+1])
+ *   diag_state  diag_words        computational-basis state, one bit per unit;
+ *                                 NULL = no expectation value
+ *   n_terms_out n_gates           live terms after each gate (may be NULL)
+ */
+int pq_run(pq_engine* engine, const pq_run_config* cfg, const uint64_t* obs_words,
+           const double* obs_coeffs, size_t n_obs, const uint64_t* gate_words,
+           const double* gate_angles, size_t n_gates, const uint32_t* layer_offsets,
+           size_t n_layers, const uint64_t* diag_state, size_t diag_words,
+           uint64_t* n_terms_out, pq_result* out);
+
+/* Final terms of the last run with want_terms, with the deferred Clifford
+ * frame applied and its sign folded into the coefficient
+ * (crates/pauli/src/engine.rs:216-224, partitioned_termsum.rs:265-272).
+ * Writes min(cap, n) terms, returns n. */
+size_t pq_result_terms(pq_engine* engine, uint64_t* keys, double* coeffs, size_t cap);
+
+/* Plugins: the reference's loader and validation, byte for byte the same
+ * symbol names (crates/core/src/policy/native_noise.rs:217-288,
+ * crates/core/src/policy/native_truncator.rs:205-276). */
+int pq_plugin_load_noise(const char* path, const char* config_json, pq_plugin** out,
+                         char* err, size_t err_len);
+int pq_plugin_load_truncator(const char* path, const char* config_json, pq_plugin** out,
+                             char* err, size_t err_len);
+void pq_plugin_free(pq_plugin* plugin);
+uint32_t pq_plugin_depends(const pq_plugin* plugin);
+/* NativeNoiseModel.factor_term (native_noise.rs:316-333). */
+double pq_plugin_noise_factor(const pq_plugin* plugin, uint32_t basis_kind, const uint64_t* words,
+                              size_t n_words, uint32_t n_units, uint32_t weight,
+                              uint32_t layer_index, uint32_t n_layers);
+/* NativeTruncator.keep_term (native_truncator.rs:305-328); 1 = keep. */
+int pq_plugin_truncator_keep(const pq_plugin* plugin, uint32_t basis_kind, const uint64_t* words,
+                             size_t n_words, uint32_t n_units, uint32_t weight,
+                             double coeff_magnitude, uint32_t layer_index, uint32_t n_layers);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PROPAQ_CUDA_H */

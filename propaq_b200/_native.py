@@ -1,0 +1,249 @@
+"""ctypes binding of libpropaq_cuda.so (declared in include/propaq_cuda.h).
+
+This is the only module that touches the CUDA engine.  There is no CPU
+fallback: if the library is missing or no CUDA device is present, every
+propagation call raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "lib" / "libpropaq_cuda.so"
+
+PQ_OK = 0
+PQ_ERR_INVALID = 1
+PQ_ERR_CUDA = 2
+PQ_ERR_OOM = 3
+PQ_ERR_CEILING = 4
+PQ_ERR_PLUGIN_LOAD = 5
+PQ_ERR_PLUGIN = 6
+PQ_ERR_DEVICE_TIMEOUT = 7
+PQ_ERR_UNSUPPORTED = 8
+
+PQ_NOISE_NONE = 0
+PQ_NOISE_TABLE = 1
+PQ_NOISE_LAYERED = 2
+PQ_NOISE_PLUGIN = 3
+
+
+class EngineUnavailable(RuntimeError):
+    """The CUDA engine library or a CUDA device is missing."""
+
+
+class RunConfig(ctypes.Structure):
+    _fields_ = [
+        ("basis_kind", ctypes.c_uint32),
+        ("n_units", ctypes.c_uint32),
+        ("max_weight", ctypes.c_int64),
+        ("has_min_coeff", ctypes.c_uint32),
+        ("min_coeff", ctypes.c_double),
+        ("min_terms", ctypes.c_int64),
+        ("truncator", ctypes.c_void_p),
+        ("noise_kind", ctypes.c_uint32),
+        ("noise_tables", ctypes.c_void_p),
+        ("noise_table_len", ctypes.c_size_t),
+        ("noise_plugin", ctypes.c_void_p),
+        ("want_terms", ctypes.c_uint32),
+        ("profile", ctypes.c_uint32),
+    ]
+
+
+class RunResult(ctypes.Structure):
+    _fields_ = [
+        ("expectation_value", ctypes.c_double),
+        ("terms_below_cutoff", ctypes.c_uint64),
+        ("sparse_key_bytes", ctypes.c_uint64),
+        ("n_final", ctypes.c_uint64),
+        ("n_layers_run", ctypes.c_uint64),
+        ("n_gates_run", ctypes.c_uint64),
+        ("gpu_launches", ctypes.c_uint64),
+        ("peak_terms", ctypes.c_uint64),
+        ("device_ms", ctypes.c_double),
+        ("gate_ms", ctypes.c_double),
+        ("noise_ms", ctypes.c_double),
+        ("phase_ms", ctypes.c_double),
+        ("gate_ops", ctypes.c_uint64),
+        ("noise_ops", ctypes.c_uint64),
+        ("phase_ops", ctypes.c_uint64),
+        ("sum_rows_gate", ctypes.c_uint64),
+        ("sum_anti", ctypes.c_uint64),
+        ("sum_children", ctypes.c_uint64),
+        ("sum_rows_noise", ctypes.c_uint64),
+        ("sum_kept", ctypes.c_uint64),
+    ]
+
+
+_V = ctypes.c_void_p
+_Z = ctypes.c_size_t
+_U32 = ctypes.c_uint32
+
+_SIGNATURES = {
+    "pq_words_for_units": (_U32, [_U32]),
+    "pq_engine_create": (ctypes.c_int, [ctypes.POINTER(_V), ctypes.c_int]),
+    "pq_engine_destroy": (None, [_V]),
+    "pq_engine_last_error": (ctypes.c_char_p, [_V]),
+    "pq_run": (ctypes.c_int, [_V, ctypes.POINTER(RunConfig), _V, _V, _Z, _V, _V, _Z, _V, _Z, _V, _Z, _V,
+                              ctypes.POINTER(RunResult)]),
+    "pq_result_terms": (_Z, [_V, _V, _V, _Z]),
+    "pq_plugin_load_noise": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_V),
+                                            ctypes.c_char_p, _Z]),
+    "pq_plugin_load_truncator": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_V),
+                                                ctypes.c_char_p, _Z]),
+    "pq_plugin_free": (None, [_V]),
+    "pq_plugin_depends": (_U32, [_V]),
+    "pq_plugin_noise_factor": (ctypes.c_double, [_V, _U32, _V, _Z, _U32, _U32, _U32, _U32]),
+    "pq_plugin_truncator_keep": (ctypes.c_int, [_V, _U32, _V, _Z, _U32, _U32, ctypes.c_double, _U32, _U32]),
+}
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def library_path() -> Path:
+    return _LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libpropaq_cuda.so (built in-tree by propaq_b200.build)."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not _LIB_PATH.exists():
+                raise EngineUnavailable(
+                    f"{_LIB_PATH} is missing: build it with `python -m propaq_b200.build` "
+                    "(there is no CPU fallback)"
+                )
+            handle = ctypes.CDLL(str(_LIB_PATH))
+            for name, (res, args) in _SIGNATURES.items():
+                fn = getattr(handle, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = handle
+        return _lib
+
+
+def words_for_units(n_units: int) -> int:
+    return int(lib().pq_words_for_units(n_units))
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Engine:
+    """One CUDA engine (device memory + stream) on one device."""
+
+    def __init__(self, device: int = 0):
+        handle = ctypes.c_void_p()
+        rc = lib().pq_engine_create(ctypes.byref(handle), device)
+        if rc != PQ_OK:
+            raise EngineUnavailable(f"no usable CUDA device {device} for the propagation engine (code {rc})")
+        self._h = handle
+        self.device = device
+        self.lock = threading.Lock()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.pq_engine_destroy(h)
+            self._h = None
+
+    def run(self, cfg: RunConfig, obs_words, obs_coeffs, gate_words, gate_angles, layer_offsets,
+            diag_state=None, want_n_terms=True):
+        """Runs pq_run; returns (RunResult, n_terms array or None)."""
+        obs_words = np.ascontiguousarray(obs_words, dtype=np.uint64)
+        obs_coeffs = np.ascontiguousarray(obs_coeffs, dtype=np.float64)
+        gate_words = np.ascontiguousarray(gate_words, dtype=np.uint64)
+        gate_angles = np.ascontiguousarray(gate_angles, dtype=np.float64)
+        layer_offsets = np.ascontiguousarray(layer_offsets, dtype=np.uint32)
+        n_gates = len(gate_angles)
+        nt = np.zeros(n_gates, dtype=np.uint64) if want_n_terms else None
+        diag = None if diag_state is None else np.ascontiguousarray(diag_state, dtype=np.uint64)
+        res = RunResult()
+        with self.lock:
+            rc = lib().pq_run(self._h, ctypes.byref(cfg), _ptr(obs_words), _ptr(obs_coeffs), len(obs_coeffs),
+                              _ptr(gate_words), _ptr(gate_angles), n_gates, _ptr(layer_offsets),
+                              len(layer_offsets) - 1, _ptr(diag), 0 if diag is None else len(diag), _ptr(nt),
+                              ctypes.byref(res))
+            if rc != PQ_OK:
+                raise_for(rc, lib().pq_engine_last_error(self._h).decode(errors="replace"))
+        return res, nt
+
+    def terms(self, n_words: int):
+        """Final (keys, coeffs) of the last run made with want_terms."""
+        with self.lock:
+            n = lib().pq_result_terms(self._h, None, None, 0)
+            keys = np.zeros((n, n_words), dtype=np.uint64)
+            coeffs = np.zeros(n, dtype=np.float64)
+            if n:
+                lib().pq_result_terms(self._h, _ptr(keys), _ptr(coeffs), n)
+        return keys, coeffs
+
+
+def raise_for(code: int, message: str):
+    if code in (PQ_ERR_INVALID, PQ_ERR_PLUGIN):
+        raise ValueError(message)
+    if code == PQ_ERR_PLUGIN_LOAD:
+        raise OSError(message)
+    if code == PQ_ERR_OOM:
+        raise MemoryError(message)
+    if code == PQ_ERR_UNSUPPORTED:
+        raise NotImplementedError(message)
+    raise RuntimeError(message)
+
+
+_engines: dict[int, Engine] = {}
+_engines_lock = threading.Lock()
+
+
+def engine(device: int = 0) -> Engine:
+    """The process-wide engine for a device (created on first use)."""
+    with _engines_lock:
+        e = _engines.get(device)
+        if e is None:
+            e = Engine(device)
+            _engines[device] = e
+        return e
+
+
+class Plugin:
+    """A loaded native noise / truncation plugin (owned; freed on collection)."""
+
+    def __init__(self, path: str, config: str | None, noise: bool):
+        handle = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(1024)
+        fn = lib().pq_plugin_load_noise if noise else lib().pq_plugin_load_truncator
+        rc = fn(str(path).encode(), None if config is None else config.encode(), ctypes.byref(handle), err, 1024)
+        if rc != PQ_OK:
+            raise_for(rc, err.value.decode(errors="replace"))
+        self._h = handle
+        self.noise = noise
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    @property
+    def depends(self) -> int:
+        return int(lib().pq_plugin_depends(self._h))
+
+    def factor(self, basis_kind, words, n_units, weight, layer_index=0, n_layers=0) -> float:
+        w = np.ascontiguousarray(list(words), dtype=np.uint64)
+        return float(lib().pq_plugin_noise_factor(self._h, basis_kind, _ptr(w) if len(w) else None, len(w),
+                                                  n_units, weight, layer_index, n_layers))
+
+    def keep(self, basis_kind, words, n_units, weight, coeff_magnitude, layer_index=0, n_layers=0) -> bool:
+        w = np.ascontiguousarray(list(words), dtype=np.uint64)
+        return bool(lib().pq_plugin_truncator_keep(self._h, basis_kind, _ptr(w) if len(w) else None, len(w),
+                                                   n_units, weight, coeff_magnitude, layer_index, n_layers))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.pq_plugin_free(h)
+            self._h = None

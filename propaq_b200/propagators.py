@@ -1,0 +1,227 @@
+"""PauliPropagator / MajoranaPropagator: the reference's propagator surface
+(crates/pauli/src/propagator.rs:117-426, crates/majorana/src/propagator.rs,
+propaq/_rust_core/__init__.pyi:225-277, :502-560) over the CUDA engine.
+
+`n_threads` and `pin_threads` are accepted for API compatibility; the engine
+runs on one GPU and has no host worker pool.
+"""
+
+from __future__ import annotations
+
+import json
+
+import numpy as np
+
+from . import _native
+from .datatypes import MajoranaMonomial, MajoranaTermSum, PauliString, PauliTermSum, words_to_int
+from .noise import NativeNoiseModel, resolve_noise
+from .truncation import reject_surrogate_only, resolve_config, resolve_truncation
+
+MAX_UNITS = 2048
+
+
+class PropagationResult:
+    """crates/core/src/interface/results.rs:8-51."""
+
+    def __init__(self, expectation_value: float, n_terms, sparse_key_bytes: int = 0, terms_below_cutoff: int = 0):
+        self.expectation_value = float(expectation_value)
+        self.n_terms = list(n_terms)
+        self.sparse_key_bytes = int(sparse_key_bytes)
+        self.terms_below_cutoff = int(terms_below_cutoff)
+
+    def __repr__(self):
+        return (f"PropagationResult(expectation_value={self.expectation_value}, n_terms=[{len(self.n_terms)} gates], "
+                f"sparse_key_bytes={self.sparse_key_bytes}, terms_below_cutoff={self.terms_below_cutoff})")
+
+
+class Logger:
+    """JSON-lines run log (crates/core/src/interface/logger.rs:19)."""
+
+    def __init__(self, filename: str, log_every: int = 1):
+        self.filename = filename
+        self.log_every = max(1, int(log_every))
+
+
+def heisenberg_gates(circuit, n_words: int, key_of):
+    """Flattens circuit.layers into arrays in Heisenberg order: layers reversed and
+    the gates within each layer reversed (crates/pauli/src/engine.rs:44-70).
+    Returns (gate_words [G, n_words], angles [G], layer_offsets [L+1])."""
+    layers = list(circuit.layers)
+    gens, angles, offsets = [], [], [0]
+    for layer in reversed(layers):
+        for rot in reversed(list(layer)):
+            gens.append(key_of(rot.generator))
+            angles.append(float(rot.angle))
+        offsets.append(len(angles))
+    g = np.zeros((len(gens), n_words), dtype=np.uint64)
+    mask = (1 << 64) - 1
+    for i, k in enumerate(gens):
+        for w in range(n_words):
+            g[i, w] = (k >> (64 * w)) & mask
+    return g, np.array(angles, dtype=np.float64), np.array(offsets, dtype=np.uint32)
+
+
+def state_words(initial_state, n_units: int) -> np.ndarray:
+    """A computational-basis state (Python int, bit u = unit u) as u64 words."""
+    s = int(initial_state or 0)
+    if s < 0:
+        raise ValueError("initial_state must be a non-negative integer bitstring")
+    n_words = max(1, (n_units + 63) // 64)
+    mask = (1 << 64) - 1
+    return np.array([(s >> (64 * i)) & mask for i in range(n_words)], dtype=np.uint64)
+
+
+class _Propagator:
+    _basis = 0
+
+    def __init__(self, noise=None, truncation=None, n_threads=None, logger=None, pin_threads=True,
+                 progress_bar=False, progress_every=1, device: int = 0):
+        self._truncators = resolve_truncation(truncation)
+        reject_surrogate_only(self._truncators)
+        self._noise = noise
+        self.n_threads = n_threads
+        self.logger = logger
+        self.pin_threads = pin_threads
+        self.progress_bar = progress_bar
+        self.progress_every = progress_every
+        self.device = device
+        self.last_run = None  # the engine's RunResult of the latest call
+
+    @property
+    def noise(self):
+        return self._noise
+
+    def set_noise(self, noise=None):
+        self._noise = noise
+
+    @property
+    def truncators(self):
+        return list(self._truncators)
+
+    def set_truncation(self, truncation=None):
+        t = resolve_truncation(truncation)
+        reject_surrogate_only(t)
+        self._truncators = t
+
+    # --- basis hooks
+    def _n_units(self, observable) -> int:
+        raise NotImplementedError
+
+    def _width_error(self, observable):
+        raise NotImplementedError
+
+    def _key(self, term) -> int:
+        return term.key()
+
+    def _make_sum(self, keys, coeffs, observable):
+        raise NotImplementedError
+
+    def _run(self, observable, circuit, initial_state, want_terms):
+        n_units = self._n_units(observable)
+        if n_units > MAX_UNITS:
+            self._width_error(observable)
+        n_words = _native.words_for_units(n_units)
+        if n_words == 0:
+            self._width_error(observable)
+        cfg = resolve_config(self._truncators)
+        kind, tables, plugin = resolve_noise(self._noise, n_units)
+        rc = _native.RunConfig()
+        rc.basis_kind = self._basis
+        rc.n_units = n_units
+        rc.max_weight = -1 if cfg.weight is None else int(cfg.weight)
+        rc.has_min_coeff = 0 if cfg.coefficient is None else 1
+        rc.min_coeff = 0.0 if cfg.coefficient is None else float(cfg.coefficient)
+        rc.min_terms = -1 if cfg.min_terms is None else int(cfg.min_terms)
+        rc.truncator = None if cfg.native is None else cfg.native.handle
+        rc.noise_kind = kind
+        if tables is not None:
+            rc.noise_tables = tables.ctypes.data
+            rc.noise_table_len = len(tables)
+        if plugin is not None:
+            rc.noise_plugin = plugin.handle
+        rc.want_terms = 1 if want_terms else 0
+        obs_keys, obs_coeffs = observable.to_arrays(n_words)
+        gw, ga, off = heisenberg_gates(circuit, n_words, self._key)
+        diag = None if initial_state is None else state_words(initial_state, n_units)
+        eng = _native.engine(self.device)
+        res, nt = eng.run(rc, obs_keys, obs_coeffs, gw, ga, off, diag)
+        self.last_run = res
+        terms = eng.terms(n_words) if want_terms else None
+        if self.logger is not None:
+            self._write_log(res, nt, n_units)
+        return res, nt, terms, n_words
+
+    def _write_log(self, res, nt, n_units):
+        with open(self.logger.filename, "a") as f:
+            for g, n in enumerate(nt):
+                if g % self.logger.log_every == 0:
+                    f.write(json.dumps({"event": "gate", "gate_idx": g, "terms_after": int(n)}) + "\n")
+            f.write(json.dumps({"event": "engine_phases", "terms": int(res.n_final), "peak_terms": int(res.peak_terms),
+                                "device_ms": res.device_ms, "gpu_launches": int(res.gpu_launches),
+                                "n_units": n_units}) + "\n")
+
+    def propagate(self, observable, circuit, filename=None):
+        """Back-propagates `observable` through `circuit`; returns the evolved term sum."""
+        res, nt, terms, n_words = self._run(observable, circuit, None, True)
+        keys, coeffs = terms
+        out = self._make_sum(keys, coeffs, observable)
+        if filename is not None:
+            from .term_io import save_terms
+
+            save_terms(filename, keys, coeffs, self._basis, self._n_units_io(observable))
+        return out
+
+    def expectation_value(self, observable, circuit, initial_state=None, filename=None) -> PropagationResult:
+        """<initial_state| U^dag O U |initial_state> via Heisenberg propagation."""
+        res, nt, terms, n_words = self._run(observable, circuit, 0 if initial_state is None else initial_state,
+                                            filename is not None)
+        if filename is not None:
+            from .term_io import save_terms
+
+            save_terms(filename, terms[0], terms[1], self._basis, self._n_units_io(observable))
+        return PropagationResult(res.expectation_value, [int(x) for x in nt], res.sparse_key_bytes,
+                                 res.terms_below_cutoff)
+
+    def _n_units_io(self, observable) -> int:
+        return observable.n_units()
+
+
+class PauliPropagator(_Propagator):
+    """Back-propagates Pauli observables through circuits of Pauli rotations on the GPU."""
+
+    _basis = 0
+
+    def _n_units(self, observable) -> int:
+        if not isinstance(observable, PauliTermSum):
+            raise TypeError("observable must be a PauliTermSum")
+        return observable.n_units()
+
+    def _width_error(self, observable):
+        raise ValueError(f"propaq: {observable.n_units()} qubits exceeds the engine's maximum of {MAX_UNITS}")
+
+    def _make_sum(self, keys, coeffs, observable):
+        return PauliTermSum.from_arrays(keys, coeffs, observable.n_units())
+
+
+class MajoranaPropagator(_Propagator):
+    """Back-propagates Majorana observables through circuits of Majorana rotations on the GPU."""
+
+    _basis = 1
+
+    def _n_units(self, observable) -> int:
+        if not isinstance(observable, MajoranaTermSum):
+            raise TypeError("observable must be a MajoranaTermSum")
+        n_modes = observable.n_units()
+        if n_modes % 2:
+            self._width_error(observable)
+        return n_modes // 2
+
+    def _width_error(self, observable):
+        raise ValueError(f"propaq: {observable.n_units()} qubits exceeds the engine's maximum of {MAX_UNITS}")
+
+    def _make_sum(self, keys, coeffs, observable):
+        return MajoranaTermSum.from_arrays(keys, coeffs, observable.n_units())
+
+
+__all__ = ["PauliPropagator", "MajoranaPropagator", "PropagationResult", "Logger", "heisenberg_gates",
+           "state_words", "PauliString", "MajoranaMonomial", "words_to_int", "NativeNoiseModel"]

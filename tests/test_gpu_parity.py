@@ -1,0 +1,285 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle.
+
+Term sets must match bit for bit and every coefficient must be identical:
+each merge in the reference is one two-operand FP64 add whose operands do not
+depend on processing order (K -> G.K is an involution), so the engine
+reproduces every coefficient exactly.  Only the expectation value is a sum
+whose rounding depends on order; it is compared against the oracle's
+compensated sum at 1e-12 relative (harness.expectation_close).
+"""
+
+import math
+
+import numpy as np
+import pytest
+from harness import (
+    Problem,
+    assert_terms_equal,
+    expectation_close,
+    from_circuit,
+    from_workload,
+    golden_fixture,
+    golden_problem,
+    run_gpu,
+    run_oracle,
+)
+from oracle_client import REF_PLUGINS
+from plugin_build import build_all
+
+import propaq_b200 as pq
+from propaq_b200 import workloads
+from propaq_b200.circuits import MajoranaCircuit, MajoranaRotation, PauliCircuit, PauliRotation
+from propaq_b200.datatypes import MajoranaMonomial, MajoranaTermSum, PauliString, PauliTermSum
+
+pytestmark = pytest.mark.gpu
+
+
+def check(engine, oracle, p: Problem, parts=1):
+    g = run_gpu(engine, p)
+    o = run_oracle(oracle, p, n_partitions=parts)
+    assert np.array_equal(g.n_terms, o.n_terms), "live counts per gate differ"
+    assert_terms_equal(g.keys, g.coeffs, o.keys, o.coeffs)
+    assert g.terms_below_cutoff == o.terms_below_cutoff
+    if p.diag is not None:
+        ok, err, tol = expectation_close(g.expectation, o)
+        assert ok, f"expectation {g.expectation!r} vs oracle {o.expectation_accurate!r} (err {err:.3g} > {tol:.3g})"
+    return g, o
+
+
+# ------------------------------------------------------------ golden circuit
+GOLD = [c for c in golden_fixture()["cases"] if "plugin" not in c]
+
+
+@pytest.mark.parametrize("case", GOLD, ids=[c["name"] for c in GOLD])
+def test_golden_builtin(gpu_engine, oracle, case):
+    p = golden_problem(max_weight=case.get("max_weight"), min_coeff=case.get("min_coeff"))
+    if "noise" in case:
+        d = case["noise"]["uniform"]
+        p.noise_table = np.array([math.exp(-d * float(w)) for w in range(p.n_units + 1)])
+    g, o = check(gpu_engine, oracle, p)
+    assert abs(g.expectation - case["expected"]) <= 1e-12 * abs(case["expected"])
+
+
+def test_golden_through_propagator_api(gpu_engine):
+    fx = golden_fixture()
+    n = fx["n_qubits"]
+    circ = pq.PauliCircuit([pq.PauliRotation(PauliString(r["x"], r["z"], n), r["angle"]) for r in fx["rotations"]])
+    obs = pq.PauliTermSum()
+    obs.add(PauliString(0, 1, n), 1.0)
+    for case in GOLD:
+        trunc = []
+        if case.get("max_weight") is not None:
+            trunc.append(pq.WeightTruncator(case["max_weight"]))
+        if case.get("min_coeff") is not None:
+            trunc.append(pq.CoefficientTruncator(case["min_coeff"]))
+        noise = pq.UniformNoiseModel(case["noise"]["uniform"]) if "noise" in case else None
+        prop = pq.PauliPropagator(noise=noise, truncation=trunc, n_threads=4)
+        res = prop.expectation_value(obs, circ, initial_state=0)
+        assert abs(res.expectation_value - case["expected"]) <= 1e-12 * abs(case["expected"])
+        assert len(res.n_terms) == 40
+
+
+@pytest.fixture(scope="module")
+def test_plugins(tmp_path_factory):
+    return build_all(tmp_path_factory.mktemp("gpu_plugins"))
+
+
+@pytest.mark.parametrize("name", ["uniform", "layered"])
+def test_weight_only_plugins_match_oracle(gpu_engine, oracle, test_plugins, name):
+    # A plugin that does not read keys is tabulated by weight (per layer when
+    # it reads the layer), noise_resolver.rs:78-131.
+    p = golden_problem(max_weight=3, min_coeff=1e-4)
+    cfg = '{"damping": 0.03}'
+    g_plugin = pq.NativeNoiseModel(str(test_plugins[name]), cfg)
+    o_plugin = oracle.load_plugin(test_plugins[name], cfg, noise=True)
+    try:
+        g = run_gpu(gpu_engine, p, noise_plugin=g_plugin.handle)
+        o = oracle.run(p.basis, p.n_units, p.n_words, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets,
+                       max_weight=3, min_coeff=1e-4, noise_plugin=o_plugin, diag_state=p.diag)
+    finally:
+        oracle.lib.pqo_plugin_free(o_plugin)
+    assert np.array_equal(g.n_terms, o.n_terms)
+    assert_terms_equal(g.keys, g.coeffs, o.keys, o.coeffs)
+
+
+@pytest.mark.parametrize("case", [c for c in golden_fixture()["cases"]
+                                  if c.get("plugin") in ("uniform_noise", "thermal_decay_noise", "drifting_noise",
+                                                         "depth_dependent_noise")],
+                         ids=lambda c: c["name"])
+def test_reference_weight_only_plugins_golden(gpu_engine, case):
+    so = REF_PLUGINS / f"{case['plugin']}.so"
+    if not so.exists():
+        pytest.skip("reference example plugins not built")
+    p = golden_problem()
+    m = pq.NativeNoiseModel(str(so), case["plugin_config"])
+    g = run_gpu(gpu_engine, p, noise_plugin=m.handle)
+    assert abs(g.expectation - case["expected"]) <= 1e-12 * abs(case["expected"])
+
+
+def test_key_reading_plugins_are_refused(gpu_engine, test_plugins):
+    obs = pq.PauliTermSum({PauliString(0, 1, 4): 1.0})
+    circ = pq.PauliCircuit([pq.PauliRotation(PauliString(1, 0, 4), 0.3)])
+    prop = pq.PauliPropagator(noise=pq.NativeNoiseModel(str(test_plugins["keyed"]), '{"damping": 0.1}'))
+    with pytest.raises(NotImplementedError):
+        prop.expectation_value(obs, circ, 0)
+
+
+# ------------------------------------------------------------ random circuits
+def random_pauli_problem(seed, n, n_gates=60, layer_size=4, clifford_frac=0.15, **kw):
+    rng = np.random.default_rng(seed)
+    layers, layer = [], []
+    for _ in range(n_gates):
+        k = int(rng.integers(1, 4))
+        qs = rng.choice(n, size=k, replace=False)
+        x = z = 0
+        for q in qs:
+            t = int(rng.integers(1, 4))
+            x |= (t & 1) << int(q)
+            z |= (t >> 1) << int(q)
+        r = rng.random()
+        if r < clifford_frac:
+            a = float(rng.choice([math.pi / 2, -math.pi / 2, 3 * math.pi / 2]))
+        elif r < clifford_frac + 0.05:
+            a = math.pi
+        else:
+            a = float(rng.uniform(-1.2, 1.2))
+        layer.append(PauliRotation(PauliString(x, z, n), a))
+        if len(layer) == layer_size:
+            layers.append(layer)
+            layer = []
+    if layer:
+        layers.append(layer)
+    obs = PauliTermSum()
+    for _ in range(3):
+        q = int(rng.integers(0, n))
+        obs.add(PauliString(0, 1 << q, n), float(rng.normal()))
+    obs.add(PauliString(0, (1 << int(rng.integers(0, n))) | 1, n), 0.5)
+    return from_circuit(0, n, obs, PauliCircuit(layers), int(rng.integers(0, 1 << min(n, 62))), **kw)
+
+
+PAULI_CASES = [
+    dict(n=6),
+    dict(n=6, min_coeff=1e-3),
+    dict(n=12, max_weight=4, min_coeff=1e-4),
+    dict(n=20, max_weight=5, min_coeff=1e-5, min_terms=200),
+    dict(n=40, max_weight=6, min_coeff=1e-4),       # W = 2
+    dict(n=70, max_weight=6, min_coeff=1e-4),       # W = 4
+    dict(n=130, max_weight=5, min_coeff=1e-3),      # W = 8
+    dict(n=33, clifford_frac=0.5, max_weight=5),    # deferral-heavy, W = 2
+]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+@pytest.mark.parametrize("case", PAULI_CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+def test_random_pauli(gpu_engine, oracle, case, seed):
+    case = dict(case)
+    n = case.pop("n")
+    cf = case.pop("clifford_frac", 0.15)
+    p = random_pauli_problem(seed, n, clifford_frac=cf, **case)
+    check(gpu_engine, oracle, p)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_random_pauli_with_noise(gpu_engine, oracle, seed):
+    p = random_pauli_problem(seed + 10, 24, n_gates=90, max_weight=5, min_coeff=1e-4)
+    p.noise_table = np.array([math.exp(-0.02 * w) for w in range(p.n_units + 1)])
+    check(gpu_engine, oracle, p)
+    q = random_pauli_problem(seed + 20, 24, n_gates=90)  # noise without truncation: scale only
+    q.noise_table = np.array([math.exp(-0.02 * w) for w in range(q.n_units + 1)])
+    check(gpu_engine, oracle, q)
+
+
+def random_majorana_problem(seed, n_sites, n_gates=50, **kw):
+    rng = np.random.default_rng(seed)
+    n_modes = 2 * n_sites
+    rots = []
+    for _ in range(n_gates):
+        kind = rng.random()
+        i, j = sorted(int(v) for v in rng.choice(n_sites, size=2, replace=False))
+        if kind < 0.4:
+            rots += pq.circuits.majorana_xx_plus_yy(i, j, float(rng.uniform(-math.pi, math.pi)), n_modes)
+        elif kind < 0.8:
+            rots += pq.circuits.majorana_cp(i, j, float(rng.normal(0, 0.5)), n_modes)
+        else:  # an odd-length generator (exercises the odd anticommutation fold)
+            m = 1 << int(rng.integers(0, n_modes))
+            rots.append(MajoranaRotation(MajoranaMonomial(m, n_modes, False), float(rng.uniform(-1, 1))))
+    layers = [rots[k:k + 5] for k in range(0, len(rots), 5)]
+    obs = MajoranaTermSum()
+    for _ in range(4):
+        s = int(rng.integers(0, n_sites))
+        obs.add(MajoranaMonomial(3 << (2 * s), n_modes), float(rng.normal()))
+    return from_circuit(1, n_sites, obs, MajoranaCircuit(layers), int(rng.integers(0, 1 << min(n_sites, 62))), **kw)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+@pytest.mark.parametrize("case", [dict(n=6), dict(n=16, max_weight=6, min_coeff=1e-4),
+                                  dict(n=32, max_weight=6, min_coeff=1e-4), dict(n=40, max_weight=5, min_coeff=1e-3)],
+                         ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+def test_random_majorana(gpu_engine, oracle, case, seed):
+    case = dict(case)
+    n = case.pop("n")
+    check(gpu_engine, oracle, random_majorana_problem(seed, n, **case))
+
+
+# ------------------------------------------------------------ configurations
+def test_config_tfim_chain(gpu_engine, oracle):
+    check(gpu_engine, oracle, from_workload(workloads.tfim_chain()))
+
+
+@pytest.mark.parametrize("shape", [(4, 4, 6), (6, 6, 8), (8, 8, 10)])
+def test_config_kicked_ising_reduced(gpu_engine, oracle, shape):
+    check(gpu_engine, oracle, from_workload(workloads.kicked_ising(*shape)), parts=4)
+
+
+def test_config_majorana_givens_reduced(gpu_engine, oracle):
+    check(gpu_engine, oracle, from_workload(workloads.majorana_givens(n_sites=16, reps=3)), parts=4)
+
+
+# ------------------------------------------------------------ edge cases
+def test_empty_observable_and_empty_circuit(gpu_engine, oracle):
+    p = from_circuit(0, 5, PauliTermSum(), PauliCircuit([PauliRotation(PauliString(1, 0, 5), 0.3)]), 0)
+    p.n_units = 5
+    check(gpu_engine, oracle, p)
+    obs = PauliTermSum({PauliString(0, 3, 5): 2.0, PauliString(1, 1, 5): -1.0})
+    check(gpu_engine, oracle, from_circuit(0, 5, obs, PauliCircuit([]), 3))
+
+
+def test_observable_truncated_at_admission_and_duplicates(gpu_engine, oracle):
+    n = 8
+    obs = PauliTermSum({PauliString(0xff, 0, n): 1.0, PauliString(1, 0, n): 1e-9, PauliString(0, 2, n): 0.5})
+    circ = PauliCircuit([PauliRotation(PauliString(2, 0, n), 0.4)])
+    check(gpu_engine, oracle, from_circuit(0, n, obs, circ, 0, max_weight=4, min_coeff=1e-6))
+    # duplicate rows in the raw arrays fold by addition in order
+    p = from_circuit(0, n, PauliTermSum({PauliString(0, 1, n): 0.1}), circ, 0)
+    p.obs_keys = np.concatenate([p.obs_keys, p.obs_keys, p.obs_keys])
+    p.obs_coeffs = np.array([0.1, 0.2, 0.3])
+    check(gpu_engine, oracle, p)
+
+
+def test_capacity_growth_and_engine_reuse(gpu_engine, oracle):
+    # 8x8 kicked Ising grows past the initial 64 Ki-row capacity; a second run on
+    # the same engine starts from a clean state and gives the same answer.
+    p = from_workload(workloads.kicked_ising(8, 8, 10))
+    a = run_gpu(gpu_engine, p)
+    b = run_gpu(gpu_engine, p)
+    assert a.res.peak_terms > 32768
+    assert np.array_equal(a.n_terms, b.n_terms)
+    assert_terms_equal(a.keys, a.coeffs, b.keys, b.coeffs)
+    assert a.expectation == b.expectation
+
+
+def test_width_errors(gpu_engine):
+    big = PauliTermSum({PauliString(0, 1, 2049): 1.0})
+    with pytest.raises(ValueError, match="exceeds the engine's maximum of 2048"):
+        pq.PauliPropagator().expectation_value(big, PauliCircuit([]), 0)
+    odd = MajoranaTermSum({MajoranaMonomial(3, 7): 1.0})
+    with pytest.raises(ValueError):
+        pq.MajoranaPropagator().expectation_value(odd, MajoranaCircuit([]), 0)
+
+
+def test_propagate_returns_oracle_terms(gpu_engine, oracle):
+    wl = workloads.tfim_chain(n=10, steps=3)
+    out = pq.PauliPropagator(truncation=wl.truncation()).propagate(wl.observable, wl.circuit)
+    o = run_oracle(oracle, from_workload(wl))
+    want = {PauliString.from_key(int(k[0]), 10): c for k, c in zip(o.keys, o.coeffs)}
+    assert dict(out.items()) == want
