@@ -11,10 +11,11 @@ coefficient cutoff 1e-5, FP64 coefficients.
              device time (CUDA events on the engine's stream, inputs resident)
     e2e    = the same metric through PauliPropagator.expectation_value with
              host inputs, host<->device copies inside the timed region
-    roofline: the gate kernel's algorithmic bytes (8W N + 16 A + (8+8W) A +
-             (8W+16) E per gate, N live rows, A anticommuting rows, E children)
-             over its event-timed duration, against the measured HBM copy
-             bandwidth.
+    roofline: the sweep kernel's algorithmic bytes over its event-timed
+             duration, against the measured HBM copy bandwidth.  Per gate:
+             8W N + 16 A + (8+8W) A + (8W+16) E (N live rows, A anticommuting
+             rows, E children); per noisy layer (8W+16)(N + kept); per
+             phase-only gate 8W N.
 
 `--impl reference` times the CPU restatement of the reference engine (the
 oracle) on the host cores instead.  With torchrun (N > 1) every rank runs an
@@ -264,7 +265,6 @@ def main():
         table = np.ascontiguousarray(prob.noise_table, dtype=np.float64)
         cfg.noise_kind, cfg.noise_tables, cfg.noise_table_len = _native.PQ_NOISE_TABLE, table.ctypes.data, len(table)
     cfg.want_terms = 0
-    cfg.profile = 1
 
     def device_step():
         return engine.run(cfg, prob.obs_keys, prob.obs_coeffs, prob.gate_keys, prob.angles, prob.offsets, prob.diag)
@@ -286,9 +286,9 @@ def main():
         settle()
         api_step()
 
-    dev_ms = gate_ms = noise_ms = 0.0
-    terms = launches = gate_ops = 0
-    galg = nalg = 0
+    dev_ms = sweep_ms = gate_ms = 0.0
+    terms = launches = sweep_launches = gate_ops = 0
+    alg_bytes = galg = 0
     e2e_s = 0.0
     e2e_terms = 0
     peak = 0
@@ -298,14 +298,17 @@ def main():
             res, nt = device_step()
             torch.cuda.synchronize()
             dev_ms += res.device_ms
+            sweep_ms += res.sweep_ms
+            gate_ms += res.gate_ms
             terms += int(nt.sum())
             launches += int(res.gpu_launches)
-            gate_ms += res.gate_ms
-            noise_ms += res.noise_ms
+            sweep_launches += int(res.sweep_launches)
             gate_ops += int(res.gate_ops)
             peak = max(peak, int(res.peak_terms))
-            galg += gate_bytes(W, res.sum_rows_gate, res.sum_anti, res.sum_children)
-            nalg += (8 * W + 16) * (res.sum_rows_noise + res.sum_kept)
+            g = gate_bytes(W, res.sum_rows_gate, res.sum_anti, res.sum_children)
+            galg += g
+            alg_bytes += (g + 8 * W * res.sum_rows_phase
+                          + (8 * W + 16) * (res.sum_rows_noise + res.sum_kept))
         for _ in range(args.steps):
             settle()
             t0 = time.perf_counter()
@@ -327,9 +330,11 @@ def main():
            + (0 if table is None else table.nbytes))
     d2h = 8 * len(prob.angles) + 16 * n_ops + 32 * 4 * 148
     peak_gbs, peak_kind = measured_peaks()
-    achieved = galg / (gate_ms / 1e3) / 1e9 if gate_ms > 0 else None
+    # The dominant kernel is the sweep: one cooperative launch per step (plus
+    # one per capacity growth) runs every gate and noise op.
+    achieved = alg_bytes / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else None
     traffic = None
-    tf = ROOT / "profiles" / f"gate_kernel_traffic_{wl.name}.json"
+    tf = ROOT / "profiles" / f"sweep_traffic_{wl.name}.json"
     if tf.exists():
         traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
     line = dict(base_line, value=value, ms_per_step=1e3 * dev_s / args.steps,
@@ -338,11 +343,13 @@ def main():
                 gpu_launches=launches,
                 roofline={"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
                           "frac": None if achieved is None else achieved / peak_gbs, "traffic": traffic,
-                          "kernel": "gate_kernel", "peak_source": f"{peak_kind} hbm_gbs",
-                          "algorithmic_bytes_per_launch": galg / max(1, gate_ops),
-                          "ms_per_launch": gate_ms / max(1, gate_ops),
-                          "share_of_device_time": gate_ms / dev_ms if dev_ms else None,
-                          "noise_kernel_gbs": nalg / (noise_ms / 1e3) / 1e9 if noise_ms > 0 else None},
+                          "kernel": "sweep_kernel", "peak_source": f"{peak_kind} hbm_gbs",
+                          "launches": sweep_launches,
+                          "algorithmic_bytes_per_launch": alg_bytes / max(1, sweep_launches),
+                          "ms_per_launch": sweep_ms / max(1, sweep_launches),
+                          "share_of_device_time": sweep_ms / dev_ms if dev_ms else None,
+                          "gate_ops_gbs": galg / (gate_ms / 1e3) / 1e9 if gate_ms > 0 else None,
+                          "us_per_gate_op": 1e3 * gate_ms / max(1, gate_ops)},
                 clocks=clocks, peak_terms=peak, expectation_value=r.expectation_value)
     line["config"]["parallelism"] = f"replicas x{world}"
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -81,7 +81,6 @@ typedef struct pq_run_config {
   size_t noise_table_len;    /* entries per table (normally n_units + 1)       */
   const pq_plugin* noise_plugin; /* PLUGIN kind                                 */
   uint32_t want_terms;       /* keep the final terms for pq_result_terms        */
-  uint32_t profile;          /* time every op with CUDA events (pq_result *_ms) */
 } pq_run_config;
 
 /* crates/core/src/interface/results.rs:8-51 (PropagationResult), plus the
@@ -94,13 +93,17 @@ typedef struct pq_result {
   uint64_t n_layers_run, n_gates_run;
   uint64_t gpu_launches;      /* kernels this run launched                    */
   uint64_t peak_terms;        /* largest live count seen                      */
-  double device_ms;           /* device time of the gate loop (CUDA events)   */
-  /* Per-kind totals; the *_ms fields are filled only with cfg->profile. */
+  double device_ms;           /* device time from the first sweep launch to the
+                                 expectation value (CUDA events, engine stream) */
+  double sweep_ms;            /* CUDA-event time of the sweep kernel launches  */
+  uint64_t sweep_launches;    /* 1, plus one per capacity growth               */
+  /* Split of the sweep time by op kind, from the device clock at each op's end. */
   double gate_ms, noise_ms, phase_ms;
   uint64_t gate_ops, noise_ops, phase_ops;
   uint64_t sum_rows_gate;     /* sum over gate ops of the live rows they scan  */
   uint64_t sum_anti;          /* ... of the rows anticommuting with the gate   */
   uint64_t sum_children;      /* ... of the children they append               */
+  uint64_t sum_rows_phase;    /* sum over phase-only ops of the rows they scan */
   uint64_t sum_rows_noise;    /* sum over noise ops of the rows they scan      */
   uint64_t sum_kept;          /* ... of the rows a reclaim keeps               */
 } pq_result;

@@ -49,7 +49,6 @@ class RunConfig(ctypes.Structure):
         ("noise_table_len", ctypes.c_size_t),
         ("noise_plugin", ctypes.c_void_p),
         ("want_terms", ctypes.c_uint32),
-        ("profile", ctypes.c_uint32),
     ]
 
 
@@ -64,6 +63,8 @@ class RunResult(ctypes.Structure):
         ("gpu_launches", ctypes.c_uint64),
         ("peak_terms", ctypes.c_uint64),
         ("device_ms", ctypes.c_double),
+        ("sweep_ms", ctypes.c_double),
+        ("sweep_launches", ctypes.c_uint64),
         ("gate_ms", ctypes.c_double),
         ("noise_ms", ctypes.c_double),
         ("phase_ms", ctypes.c_double),
@@ -73,6 +74,7 @@ class RunResult(ctypes.Structure):
         ("sum_rows_gate", ctypes.c_uint64),
         ("sum_anti", ctypes.c_uint64),
         ("sum_children", ctypes.c_uint64),
+        ("sum_rows_phase", ctypes.c_uint64),
         ("sum_rows_noise", ctypes.c_uint64),
         ("sum_kept", ctypes.c_uint64),
     ]

@@ -1,5 +1,5 @@
-// pq_device.cuh -- device-side basis algebra, key hashing and the shared
-// per-launch control block of the B200 propagation engine.
+// pq_device.cuh -- device-side basis algebra and key hashing of the B200
+// propagation engine.
 //
 // Keys are W u64 words, two bits per unit, interleaved (bit 2q = x and bit
 // 2q+1 = z of qubit q for Pauli; bit m = Majorana mode m).  All key logic is
@@ -20,27 +20,12 @@ constexpr u64 EMPTY_SLOT = ~0ULL;  // hash slot sentinel: fp 0xffffffff, row 0xf
 constexpr u32 NO_WEIGHT_CUT = 0xffffffffu;
 constexpr u32 NOT_HALTED = 0xffffffffu;
 
-// Error bits the kernels raise in Ctl::error instead of hanging or faulting.
+// Error bits the kernels raise instead of hanging or faulting.
 enum : u32 {
   ERR_LOOKBACK_TIMEOUT = 1u,  // a tile's predecessor never published its count
   ERR_PROBE_OVERFLOW = 2u,    // a hash probe ran past the table size
   ERR_CAPACITY = 4u,          // a write would have passed the row capacity
-};
-
-// Device-resident control block, one per engine.  Every persistent kernel
-// reads the live count of the current parity at entry, hands out tiles with
-// `ticket`, and the last block to leave resets the counters, publishes the
-// new count, flips the parity and advances the epoch that tags tile statuses.
-struct Ctl {
-  u32 ticket;
-  u32 done;
-  u32 epoch;
-  u32 parity;
-  u64 n[2];       // live rows, double buffered by parity
-  u64 n_next;     // new live count, written by the block owning the last tile
-  u32 halt;       // op index of the first op skipped for capacity, or NOT_HALTED
-  u32 error;      // ERR_* bits
-  u64 peak;       // largest live count seen since the last reset
+  ERR_BARRIER_TIMEOUT = 8u,   // a grid barrier wait expired
 };
 
 __host__ __device__ inline int mod4(int v) { return v & 3; }

@@ -307,11 +307,10 @@ u64 next_pow2(u64 x) {
 struct pq_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_l0 = nullptr, ev_l1 = nullptr;
   std::string err;
-  // device state
-  pq::Ctl* ctl = nullptr;
-  pq::Ctl* h_ctl = nullptr;  // pinned mirror
+  pq::SweepState* st = nullptr;    // device
+  pq::SweepState* h_st = nullptr;  // pinned mirror
   u64* keys[2] = {nullptr, nullptr};
   double* coeffs[2] = {nullptr, nullptr};
   u64* table = nullptr;
@@ -320,17 +319,21 @@ struct pq_engine {
   u64 cap = 0;
   int W = 0;
   int cur = 0;
+  u32 epoch_base = 1;
+  // per-op device arrays
+  size_t ops_cap = 0;
+  pq::OpDesc* d_ops = nullptr;
+  u32* tickets = nullptr;
   u64* hist = nullptr;
   u64* anti = nullptr;
-  size_t hist_cap = 0;
-  bool profile = false;
-  std::vector<cudaEvent_t> op_events;  // two per op when profiling
+  u64* stamps = nullptr;
+  void* d_gates = nullptr;
+  size_t gates_bytes = 0;
   double* d_tables = nullptr;
   size_t d_tables_cap = 0;
   pq::ExpectPartial* partials = nullptr;
-  int grid = 0;
-  u32 epoch_base = 1;
-  // last run's terms
+  int expect_grid = 0;
+  u32* d_err = nullptr;  // error word of the stand-alone kernels
   std::vector<u64> out_keys;
   std::vector<double> out_coeffs;
   u64 launches = 0;
@@ -340,6 +343,7 @@ struct pq_engine {
     return code;
   }
   int cuda_fail(cudaError_t e, const char* what) {
+    cudaGetLastError();
     return fail(e == cudaErrorMemoryAllocation ? PQ_ERR_OOM : PQ_ERR_CUDA,
                 std::string(what) + ": " + cudaGetErrorString(e));
   }
@@ -356,44 +360,35 @@ struct pq_engine {
     status = nullptr;
     cap = tcap = 0;
   }
+  void free_ops() {
+    for (void* p : {(void*)d_ops, (void*)tickets, (void*)hist, (void*)anti, (void*)stamps})
+      if (p) cudaFree(p);
+    d_ops = nullptr;
+    tickets = nullptr;
+    hist = anti = stamps = nullptr;
+    ops_cap = 0;
+  }
   ~pq_engine() {
     if (stream) cudaStreamSynchronize(stream);
     free_rows();
-    if (ctl) cudaFree(ctl);
-    if (h_ctl) cudaFreeHost(h_ctl);
-    if (hist) cudaFree(hist);
-    if (anti) cudaFree(anti);
-    for (auto ev : op_events) cudaEventDestroy(ev);
-    if (d_tables) cudaFree(d_tables);
-    if (partials) cudaFree(partials);
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
+    free_ops();
+    for (void* p : {(void*)st, (void*)d_gates, (void*)d_tables, (void*)partials, (void*)d_err})
+      if (p) cudaFree(p);
+    if (h_st) cudaFreeHost(h_st);
+    for (auto ev : {ev_begin, ev_end, ev_l0, ev_l1})
+      if (ev) cudaEventDestroy(ev);
     if (stream) cudaStreamDestroy(stream);
   }
-  pq::DevBufs bufs() const {
-    pq::DevBufs b;
-    b.keys = keys[cur];
-    b.coeffs = coeffs[cur];
-    b.keys_alt = keys[cur ^ 1];
-    b.coeffs_alt = coeffs[cur ^ 1];
-    b.table = table;
-    b.table_mask = tcap - 1;
-    b.cap = cap;
-    b.status = status;
-    b.ctl = ctl;
-    b.hist = hist;
-    b.anti = anti;
-    return b;
-  }
-  // (Re)allocates rows for `new_cap`, keeping the first n live rows of the
-  // current buffer in buffer 0.  The caller rebuilds the table.  Synchronous.
-  int resize(u64 new_cap, u64 n, int Wn) {
+  // (Re)allocates rows for `new_cap`, keeping the first n live rows of buffer
+  // `from` in buffer 0, then clears and rebuilds the table.  Synchronous.
+  int resize(u64 new_cap, u64 n, int from, int Wn) {
     cudaError_t e;
     u64* nk[2] = {nullptr, nullptr};
     double* nc[2] = {nullptr, nullptr};
-    u64 ntcap = 2 * new_cap;
+    const u64 ntcap = 2 * new_cap;
     u64* nt = nullptr;
     u64* ns = nullptr;
+    const u64 n_status = new_cap / TILE_ROWS + 2;
     auto cleanup = [&]() {
       for (int i = 0; i < 2; ++i) {
         if (nk[i]) cudaFree(nk[i]);
@@ -406,22 +401,22 @@ struct pq_engine {
       if ((e = cudaMalloc(&nk[i], new_cap * Wn * 8)) != cudaSuccess ||
           (e = cudaMalloc(&nc[i], new_cap * 8)) != cudaSuccess) {
         cleanup();
-        cudaGetLastError();
         return cuda_fail(e, "allocating term rows");
       }
     }
-    if ((e = cudaMalloc(&nt, ntcap * 8)) != cudaSuccess ||
-        (e = cudaMalloc(&ns, (new_cap / TILE_ROWS + 2) * 8)) != cudaSuccess) {
+    if ((e = cudaMalloc(&nt, ntcap * 8)) != cudaSuccess || (e = cudaMalloc(&ns, n_status * 8)) != cudaSuccess) {
       cleanup();
-      cudaGetLastError();
       return cuda_fail(e, "allocating the hash table");
     }
-    if (n && keys[cur]) {
-      cudaMemcpyAsync(nk[0], keys[cur], n * Wn * 8, cudaMemcpyDeviceToDevice, stream);
-      cudaMemcpyAsync(nc[0], coeffs[cur], n * 8, cudaMemcpyDeviceToDevice, stream);
+    if (n && keys[from]) {
+      cudaMemcpyAsync(nk[0], keys[from], n * Wn * 8, cudaMemcpyDeviceToDevice, stream);
+      cudaMemcpyAsync(nc[0], coeffs[from], n * 8, cudaMemcpyDeviceToDevice, stream);
     }
-    cudaMemsetAsync(ns, 0, (new_cap / TILE_ROWS + 2) * 8, stream);
-    cudaStreamSynchronize(stream);
+    cudaMemsetAsync(ns, 0, n_status * 8, stream);
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+      cleanup();
+      return cuda_fail(e, "copying rows");
+    }
     free_rows();
     keys[0] = nk[0];
     keys[1] = nk[1];
@@ -433,65 +428,35 @@ struct pq_engine {
     tcap = ntcap;
     cur = 0;
     W = Wn;
-    return PQ_OK;
+    return rebuild_table(n);
   }
-  int rebuild_table() {
+  int rebuild_table(u64 n) {
     cudaMemsetAsync(table, 0xff, tcap * 8, stream);
-    pq::DevBufs b = bufs();
     cudaError_t e;
     switch (W) {
-      case 1: e = pq::launch_rebuild<1>(b, grid * 4, stream); break;
-      case 2: e = pq::launch_rebuild<2>(b, grid * 4, stream); break;
-      case 4: e = pq::launch_rebuild<4>(b, grid * 4, stream); break;
-      default: e = pq::launch_rebuild<8>(b, grid * 4, stream); break;
+      case 1: e = pq::launch_rebuild<1>(keys[cur], n, table, tcap - 1, d_err, stream); break;
+      case 2: e = pq::launch_rebuild<2>(keys[cur], n, table, tcap - 1, d_err, stream); break;
+      case 4: e = pq::launch_rebuild<4>(keys[cur], n, table, tcap - 1, d_err, stream); break;
+      default: e = pq::launch_rebuild<8>(keys[cur], n, table, tcap - 1, d_err, stream); break;
     }
-    ++launches;
+    if (n) ++launches;
     if (e != cudaSuccess) return cuda_fail(e, "rebuild launch");
+    return PQ_OK;
+  }
+  int ensure_ops(size_t n_ops) {
+    if (ops_cap >= n_ops) return PQ_OK;
+    free_ops();
+    cudaError_t e;
+    if ((e = cudaMalloc(&d_ops, n_ops * sizeof(pq::OpDesc))) != cudaSuccess ||
+        (e = cudaMalloc(&tickets, n_ops * 4)) != cudaSuccess || (e = cudaMalloc(&hist, n_ops * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&anti, n_ops * 8)) != cudaSuccess || (e = cudaMalloc(&stamps, n_ops * 8)) != cudaSuccess)
+      return cuda_fail(e, "allocating op arrays");
+    ops_cap = n_ops;
     return PQ_OK;
   }
 };
 
 namespace {
-
-enum OpKind { OP_GATE, OP_PHASE, OP_NOISE };
-template <int W>
-struct Op {
-  OpKind kind;
-  pq::GateArgs<W> ga;
-  pq::NoiseArgs na;
-  int cur_before;  // row buffer the op reads
-};
-
-template <int W, int ALG>
-cudaError_t launch_op_inner(pq_engine* E, Op<W>& op);
-
-template <int W, int ALG>
-cudaError_t launch_op(pq_engine* E, Op<W>& op, size_t idx) {
-  if (E->profile) cudaEventRecord(E->op_events[2 * idx], E->stream);
-  cudaError_t e = launch_op_inner<W, ALG>(E, op);
-  if (E->profile) cudaEventRecord(E->op_events[2 * idx + 1], E->stream);
-  return e;
-}
-
-template <int W, int ALG>
-cudaError_t launch_op_inner(pq_engine* E, Op<W>& op) {
-  E->cur = op.cur_before;
-  pq::DevBufs b = E->bufs();
-  ++E->launches;
-  switch (op.kind) {
-    case OP_GATE: return pq::launch_gate<W, ALG>(op.ga, b, E->grid, E->stream);
-    case OP_PHASE: return pq::launch_phase_only<W, ALG>(op.ga, b, E->grid, E->stream);
-    default: {
-      if (op.na.compact) {
-        cudaMemsetAsync(E->table, 0xff, E->tcap * 8, E->stream);
-        cudaError_t e = pq::launch_noise<W, ALG>(op.na, b, E->grid, E->stream);
-        E->cur ^= 1;
-        return e;
-      }
-      return pq::launch_noise<W, ALG>(op.na, b, E->grid, E->stream);
-    }
-  }
-}
 
 template <int W>
 pq::GenInfo<W> make_gen(int alg, const u64* g, int sign) {
@@ -527,13 +492,15 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
   const double ccut = cfg->min_coeff;
   const bool has_floor = cfg->min_terms >= 0;
   const u64 floor_terms = has_floor ? (u64)cfg->min_terms : 0;
+  cudaError_t e;
 
-  // Noise resolution (noise_resolver.rs:78-131).
+  // Noise resolution (noise_resolver.rs:78-131): one factor table per layer
+  // or one for the run.
   const Plugin* np = reinterpret_cast<const Plugin*>(cfg->noise_plugin);
-  const size_t tlen = cfg->noise_table_len ? cfg->noise_table_len : (size_t)n_units + 1;
-  std::vector<double> tables;  // n_layer_tables x tlen
+  size_t tlen = cfg->noise_table_len ? cfg->noise_table_len : (size_t)n_units + 1;
+  std::vector<double> tables;
   bool layered = false;
-  bool have_noise = cfg->noise_kind != PQ_NOISE_NONE;
+  const bool have_noise = cfg->noise_kind != PQ_NOISE_NONE;
   if (cfg->noise_kind == PQ_NOISE_TABLE) {
     if (!cfg->noise_tables || !cfg->noise_table_len) return E->fail(PQ_ERR_INVALID, "noise table missing");
     tables.assign(cfg->noise_tables, cfg->noise_tables + tlen);
@@ -545,6 +512,7 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
     if (!np) return E->fail(PQ_ERR_INVALID, "noise plugin missing");
     if (np->depends & 1)
       return E->fail(PQ_ERR_UNSUPPORTED, "key-reading noise plugins are not run by the CUDA engine yet");
+    tlen = (size_t)n_units + 1;
     auto f = (NoiseFactorFn)np->fn;
     auto tab = [&](u32 layer, u32 total) {
       for (u32 w = 0; w < n_units + 1; ++w) tables.push_back(f(np->ctx, ALG, nullptr, 0, n_units, w, layer, total));
@@ -555,10 +523,11 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
     } else {
       tab(0, 0);
     }
+  } else if (cfg->noise_kind != PQ_NOISE_NONE) {
+    return E->fail(PQ_ERR_INVALID, "unknown noise kind");
   }
   if (cfg->truncator)
     return E->fail(PQ_ERR_UNSUPPORTED, "native truncator plugins are not run by the CUDA engine yet");
-  const bool defer = true;  // no key-reading plugin reaches this point (engine.rs:101-103)
 
   // Observable admission with duplicate folding (engine.rs:104-111).
   std::vector<u64> hk;
@@ -586,130 +555,157 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
   }
   const u64 n0 = hc.size();
 
-  // Device set-up.
-  cudaError_t e;
-  u64 want_cap = next_pow2(std::max<u64>(4 * n0, 1ULL << 16));
+  // Device set-up: rows, table, op arrays, noise tables.
+  const u64 want_cap = next_pow2(std::max<u64>(4 * n0, 1ULL << 16));
   if (E->W != W || E->cap < want_cap) {
-    int rc = E->resize(std::max(want_cap, E->cap), 0, W);
-    if (rc) return rc;
+    if (int rc = E->resize(std::max(want_cap, E->cap), 0, E->cur, W)) return rc;
   }
   E->cur = 0;
   if (n0) {
     cudaMemcpyAsync(E->keys[0], hk.data(), n0 * W * 8, cudaMemcpyHostToDevice, E->stream);
     cudaMemcpyAsync(E->coeffs[0], hc.data(), n0 * 8, cudaMemcpyHostToDevice, E->stream);
   }
+  if (int rc = E->rebuild_table(n0)) return rc;
   const size_t n_ops_max = n_gates + n_layers + 1;
-  if (E->hist_cap < n_ops_max) {
-    if (E->hist) cudaFree(E->hist);
-    if (E->anti) cudaFree(E->anti);
-    E->hist = E->anti = nullptr;
-    if ((e = cudaMalloc(&E->hist, n_ops_max * 8)) != cudaSuccess) return E->cuda_fail(e, "hist");
-    if ((e = cudaMalloc(&E->anti, n_ops_max * 8)) != cudaSuccess) return E->cuda_fail(e, "anti");
-    E->hist_cap = n_ops_max;
-  }
-  cudaMemsetAsync(E->anti, 0, n_ops_max * 8, E->stream);
-  E->profile = cfg->profile != 0;
-  if (E->profile && E->op_events.size() < 2 * n_ops_max) {
-    size_t have = E->op_events.size();
-    E->op_events.resize(2 * n_ops_max);
-    for (size_t i = have; i < E->op_events.size(); ++i) cudaEventCreate(&E->op_events[i]);
+  if (int rc = E->ensure_ops(n_ops_max)) return rc;
+  const size_t gbytes = std::max<size_t>(n_gates, 1) * sizeof(pq::GateDesc<W>);
+  if (E->gates_bytes < gbytes) {
+    if (E->d_gates) cudaFree(E->d_gates);
+    E->d_gates = nullptr;
+    if ((e = cudaMalloc(&E->d_gates, gbytes)) != cudaSuccess) return E->cuda_fail(e, "gate descriptors");
+    E->gates_bytes = gbytes;
   }
   if (!tables.empty() && E->d_tables_cap < tables.size()) {
     if (E->d_tables) cudaFree(E->d_tables);
+    E->d_tables = nullptr;
     if ((e = cudaMalloc(&E->d_tables, tables.size() * 8)) != cudaSuccess) return E->cuda_fail(e, "noise tables");
     E->d_tables_cap = tables.size();
   }
   if (!tables.empty())
     cudaMemcpyAsync(E->d_tables, tables.data(), tables.size() * 8, cudaMemcpyHostToDevice, E->stream);
-  pq::Ctl c0{};
-  c0.epoch = E->epoch_base;
-  c0.n[0] = n0;
-  c0.halt = pq::NOT_HALTED;
-  c0.peak = n0;
-  cudaMemcpyAsync(E->ctl, &c0, sizeof c0, cudaMemcpyHostToDevice, E->stream);
-  if (int rc = E->rebuild_table()) return rc;
+  cudaMemsetAsync(E->anti, 0, n_ops_max * 8, E->stream);
+  if (E->epoch_base > (1u << 29)) {  // keep status tags unique: restart the epochs on a cleared array
+    E->epoch_base = 1;
+    cudaMemsetAsync(E->status, 0, (E->cap / TILE_ROWS + 2) * 8, E->stream);
+  }
 
-  std::vector<Op<W>> ops;
+  std::vector<pq::OpDesc> ops;
+  std::vector<pq::GateDesc<W>> gdesc;
   ops.reserve(n_ops_max);
-  int host_cur = 0;
+  gdesc.reserve(n_gates);
   std::vector<long> gate_op(n_gates, -1);  // latest op at or before each gate
-  std::vector<long> noise_op_of_layer(n_layers, -1);
+  u64 n_live = n0, peak = n0;
+  size_t done = 0;  // ops executed so far
+  size_t gdone = 0; // gate descriptors uploaded so far
+  const int grid = pq::sweep_grid<W, ALG>();
+  double sweep_ms = 0;
+  u64 sweep_launches = 0;
 
-  // Synchronise; on a capacity halt grow, rebuild and replay from the halted op.
-  auto sync_heal = [&]() -> int {
-    for (;;) {
-      cudaMemcpyAsync(E->h_ctl, E->ctl, sizeof(pq::Ctl), cudaMemcpyDeviceToHost, E->stream);
-      if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "device");
-      const pq::Ctl h = *E->h_ctl;
-      E->epoch_base = h.epoch;
+  // Runs ops [done, ops.size()) on the device; on a capacity halt grows the
+  // rows and relaunches from the halted op.
+  auto flush = [&]() -> int {
+    if (ops.size() > done) {
+      cudaMemcpyAsync(E->d_ops + done, ops.data() + done, (ops.size() - done) * sizeof(pq::OpDesc),
+                      cudaMemcpyHostToDevice, E->stream);
+    }
+    if (gdesc.size() > gdone) {
+      cudaMemcpyAsync(reinterpret_cast<pq::GateDesc<W>*>(E->d_gates) + gdone, gdesc.data() + gdone,
+                      (gdesc.size() - gdone) * sizeof(pq::GateDesc<W>), cudaMemcpyHostToDevice, E->stream);
+      gdone = gdesc.size();
+    }
+    while (done < ops.size()) {
+      pq::SweepState s{};
+      s.n[done & 1] = n_live;
+      s.peak = peak;
+      s.halt = pq::NOT_HALTED;
+      s.bar_gen = 0;
+      *E->h_st = s;
+      cudaMemcpyAsync(E->st, E->h_st, sizeof s, cudaMemcpyHostToDevice, E->stream);
+      cudaMemsetAsync(E->tickets + done, 0, (ops.size() - done) * 4, E->stream);
+      pq::SweepArgs a{};
+      a.ops = E->d_ops;
+      a.gates = E->d_gates;
+      a.tables = E->d_tables;
+      a.table_len = (u32)tlen;
+      a.n_units = n_units;
+      a.op_begin = (u32)done;
+      a.op_end = (u32)ops.size();
+      a.cur0 = (u32)E->cur;
+      a.epoch_base = E->epoch_base;
+      a.max_weight = wcut;
+      a.has_min_coeff = has_c;
+      a.min_coeff = ccut;
+      a.min_terms = floor_terms;
+      for (int i = 0; i < 2; ++i) {
+        a.keys[i] = E->keys[i];
+        a.coeffs[i] = E->coeffs[i];
+      }
+      a.table = E->table;
+      a.table_mask = E->tcap - 1;
+      a.cap = E->cap;
+      a.status = E->status;
+      a.tickets = E->tickets;
+      a.hist = E->hist;
+      a.anti = E->anti;
+      a.stamps = E->stamps;
+      a.st = E->st;
+      cudaEventRecord(E->ev_l0, E->stream);
+      if ((e = pq::launch_sweep<W, ALG>(a, grid, E->stream)) != cudaSuccess) return E->cuda_fail(e, "sweep launch");
+      cudaEventRecord(E->ev_l1, E->stream);
+      ++E->launches;
+      ++sweep_launches;
+      E->epoch_base += (u32)ops.size() + 1;
+      cudaMemcpyAsync(E->h_st, E->st, sizeof s, cudaMemcpyDeviceToHost, E->stream);
+      if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "sweep");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, E->ev_l0, E->ev_l1);
+      sweep_ms += ms;
+      const pq::SweepState h = *E->h_st;
+      if (h.error & pq::ERR_BARRIER_TIMEOUT)
+        return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a grid barrier wait expired on the device");
       if (h.error & pq::ERR_LOOKBACK_TIMEOUT)
         return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a tile's look-back wait expired on the device");
-      if (h.error)
-        return E->fail(PQ_ERR_CUDA, "device reported error bits " + std::to_string(h.error));
-      if (h.halt == pq::NOT_HALTED) return PQ_OK;
-      const u64 n = h.n[h.parity];
-      const size_t p = h.halt;
-      const int cur_at = ops[p].cur_before;
-      u64 ncap = next_pow2(std::max<u64>(4 * n, 2 * E->cap));
-      if (ncap > MAX_ROWS) ncap = MAX_ROWS;
-      if (2 * n > ncap)
-        return E->fail(PQ_ERR_CEILING, "term index ceiling reached: " + std::to_string(2 * n) +
-                                           " rows would exceed the engine's capacity");
-      E->cur = cur_at;
-      int rc = E->resize(ncap, n, W);
-      if (rc == PQ_ERR_OOM) {  // retry with the minimum that still fits
-        ncap = next_pow2(2 * n);
-        rc = E->resize(ncap, n, W);
+      if (h.error) return E->fail(PQ_ERR_CUDA, "device reported error bits " + std::to_string(h.error));
+      E->cur = (int)h.cur;
+      done = h.end_op;
+      n_live = h.n[done & 1];
+      peak = std::max(peak, h.peak);
+      if (h.halt != pq::NOT_HALTED) {  // grow: the gate at `done` needs 2 N rows
+        u64 ncap = next_pow2(std::max<u64>(4 * n_live, 2 * E->cap));
+        if (ncap > MAX_ROWS) ncap = MAX_ROWS;
+        if (2 * n_live > ncap)
+          return E->fail(PQ_ERR_CEILING, "term index ceiling reached: " + std::to_string(2 * n_live) +
+                                             " rows would exceed the engine's capacity");
+        int rc = E->resize(ncap, n_live, E->cur, W);
+        if (rc == PQ_ERR_OOM) rc = E->resize(next_pow2(2 * n_live), n_live, E->cur, W);
+        if (rc) return rc;
       }
-      if (rc) return rc;
-      // The rows now live in buffer 0 of the new allocation: shift the
-      // recorded buffer of every op still to run, and the host's cursor.
-      pq::Ctl hc2 = h;
-      hc2.halt = pq::NOT_HALTED;
-      hc2.ticket = hc2.done = 0;
-      cudaMemcpyAsync(E->ctl, &hc2, sizeof hc2, cudaMemcpyHostToDevice, E->stream);
-      if ((rc = E->rebuild_table())) return rc;
-      for (size_t i = p; i < ops.size(); ++i) ops[i].cur_before ^= cur_at;
-      host_cur ^= cur_at;
-      for (size_t i = p; i < ops.size(); ++i)
-        if ((e = launch_op<W, ALG>(E, ops[i], i)) != cudaSuccess) return E->cuda_fail(e, "launch");
     }
+    return PQ_OK;
   };
 
-  cudaEventRecord(E->ev0, E->stream);
+  cudaEventRecord(E->ev_begin, E->stream);
   Tableau frame(ALG, W, n_units);
   std::vector<u64> g(W), gc(W);
   long last_op = -1;
   for (size_t l = 0; l < n_layers; ++l) {
     if (have_noise) {
-      Op<W> op{};
-      op.kind = OP_NOISE;
-      op.na.factors = E->d_tables + (layered ? l * tlen : 0);
-      op.na.table_len = (u32)tlen;
-      op.na.n_units = n_units;
-      op.na.max_weight = wcut;
-      op.na.has_min_coeff = has_c;
-      op.na.min_coeff = ccut;
-      op.na.compact = (has_w || has_c) ? 1u : 0u;  // partitioned_termsum.rs:585-587
-      op.na.op = (u32)ops.size();
-      op.cur_before = host_cur;
-      ops.push_back(op);
-      if ((e = launch_op<W, ALG>(E, ops.back(), ops.size() - 1)) != cudaSuccess) return E->cuda_fail(e, "launch");
-      if (op.na.compact) host_cur ^= 1;
+      pq::OpDesc od;
+      od.kind = (has_w || has_c) ? pq::OP_NOISE_COMPACT : pq::OP_NOISE_SCALE;  // partitioned_termsum.rs:585-587
+      od.idx = layered ? (u32)l : 0u;
+      ops.push_back(od);
       last_op = (long)ops.size() - 1;
-      noise_op_of_layer[l] = last_op;
     }
     for (u32 gi = layer_off[l]; gi < layer_off[l + 1]; ++gi) {
       std::memcpy(g.data(), gate_words + (size_t)gi * W, 8 * W);
       const double ang = angles[gi];
-      if (defer && std::fabs(std::cos(ang)) < EPS_CLASSIFY) {
+      if (std::fabs(std::cos(ang)) < EPS_CLASSIFY) {  // Clifford: defer into the frame when allowed
         Tableau step = Tableau::for_rotation(ALG, W, n_units, g.data(), ang);
         bool eff_w = has_w;
         const bool cw = step.changes_weight();
-        if (has_w && cw && has_floor) {  // the effective cutoff depends on the live count
-          if (int rc = sync_heal()) return rc;
-          const u64 n = E->h_ctl->n[E->h_ctl->parity];
-          if (n < floor_terms) eff_w = false;
+        if (has_w && cw && has_floor) {  // the effective cutoff depends on the live count here
+          if (int rc = flush()) return rc;
+          if (n_live < floor_terms) eff_w = false;
         }
         if (!eff_w || !cw) {
           frame.compose(step);
@@ -717,74 +713,57 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
           continue;
         }
       }
-      int sign = frame.conjugate_generator(g.data(), gc.data());
-      Op<W> op{};
-      op.ga.g = make_gen<W>(ALG, gc.data(), sign);
-      op.ga.sn = std::sin(ang);
-      op.ga.cs = std::cos(ang);
-      op.ga.max_weight = wcut;
-      op.ga.has_min_coeff = has_c;
-      op.ga.min_coeff = ccut;
-      op.ga.min_terms = floor_terms;
-      op.ga.n_units = n_units;
-      op.ga.op = (u32)ops.size();
-      op.kind = std::fabs(op.ga.sn) < EPS_CLASSIFY ? OP_PHASE : OP_GATE;
-      op.cur_before = host_cur;
-      ops.push_back(op);
-      if ((e = launch_op<W, ALG>(E, ops.back(), ops.size() - 1)) != cudaSuccess) return E->cuda_fail(e, "launch");
+      const int sign = frame.conjugate_generator(g.data(), gc.data());
+      pq::GateDesc<W> gd;
+      gd.g = make_gen<W>(ALG, gc.data(), sign);
+      gd.sn = std::sin(ang);
+      gd.cs = std::cos(ang);
+      pq::OpDesc od;
+      od.kind = std::fabs(gd.sn) < EPS_CLASSIFY ? pq::OP_PHASE : pq::OP_GATE;
+      od.idx = (u32)gdesc.size();
+      gdesc.push_back(gd);
+      ops.push_back(od);
       last_op = (long)ops.size() - 1;
       gate_op[gi] = last_op;
     }
   }
-  if (int rc = sync_heal()) return rc;
-  cudaEventRecord(E->ev1, E->stream);
-  E->cur = host_cur;
-  // After heals, the buffer index of the end state is the recorded one of a
-  // virtual op after the last: recompute from the final ctl + ops.
-  if (!ops.empty()) {
-    const Op<W>& lo = ops.back();
-    E->cur = lo.cur_before ^ ((lo.kind == OP_NOISE && lo.na.compact) ? 1 : 0);
-  }
-  const pq::Ctl hfin = *E->h_ctl;
-  const u64 n_fin = hfin.n[hfin.parity];
+  if (int rc = flush()) return rc;
+  const u64 n_fin = n_live;
 
-  std::vector<u64> hist(ops.size()), anti(ops.size());
+  std::vector<u64> hist(ops.size()), anti(ops.size()), stamps(ops.size());
   if (!ops.empty()) {
     cudaMemcpyAsync(hist.data(), E->hist, ops.size() * 8, cudaMemcpyDeviceToHost, E->stream);
     cudaMemcpyAsync(anti.data(), E->anti, ops.size() * 8, cudaMemcpyDeviceToHost, E->stream);
+    cudaMemcpyAsync(stamps.data(), E->stamps, ops.size() * 8, cudaMemcpyDeviceToHost, E->stream);
   }
 
   // Expectation value and the below-cutoff count.
   res->expectation_value = 0;
   res->terms_below_cutoff = 0;
-  std::vector<u64> fimg;
-  std::vector<int> fsgn;
   u64* d_img = nullptr;
   int* d_sgn = nullptr;
-  if (!frame.identity) {
-    fimg = frame.rd_img;
-    fsgn = frame.rd_sign;
-    if ((e = cudaMalloc(&d_img, fimg.size() * 8)) != cudaSuccess) return E->cuda_fail(e, "frame");
-    if ((e = cudaMalloc(&d_sgn, fsgn.size() * sizeof(int))) != cudaSuccess) return E->cuda_fail(e, "frame");
-    cudaMemcpyAsync(d_img, fimg.data(), fimg.size() * 8, cudaMemcpyHostToDevice, E->stream);
-    cudaMemcpyAsync(d_sgn, fsgn.data(), fsgn.size() * sizeof(int), cudaMemcpyHostToDevice, E->stream);
-  }
   struct FrameFree {
-    u64* a;
-    int* b;
+    u64** a;
+    int** b;
     ~FrameFree() {
-      if (a) cudaFree(a);
-      if (b) cudaFree(b);
+      if (*a) cudaFree(*a);
+      if (*b) cudaFree(*b);
     }
-  } ff{d_img, d_sgn};
+  } ff{&d_img, &d_sgn};
+  if (!frame.identity) {
+    if ((e = cudaMalloc(&d_img, frame.rd_img.size() * 8)) != cudaSuccess) return E->cuda_fail(e, "frame");
+    if ((e = cudaMalloc(&d_sgn, frame.rd_sign.size() * sizeof(int))) != cudaSuccess) return E->cuda_fail(e, "frame");
+    cudaMemcpyAsync(d_img, frame.rd_img.data(), frame.rd_img.size() * 8, cudaMemcpyHostToDevice, E->stream);
+    cudaMemcpyAsync(d_sgn, frame.rd_sign.data(), frame.rd_sign.size() * sizeof(int), cudaMemcpyHostToDevice,
+                    E->stream);
+  }
   if (diag || has_c) {
     pq::ExpectArgs xa{};
-    for (int i = 0; i < W; ++i) xa.state[i] = 0;
     if (diag) {
       for (u32 u = 0; u < n_units; ++u) {
-        u64 bit = (u / 64 < nd) ? (diag[u / 64] >> (u % 64)) & 1 : 0;
+        const u64 bit = (u / 64 < nd) ? (diag[u / 64] >> (u % 64)) & 1 : 0;
         if (!bit) continue;
-        u32 pos = ALG == 0 ? 2 * u + 1 : 2 * u;
+        const u32 pos = ALG == 0 ? 2 * u + 1 : 2 * u;
         if (pos / 64 < (u32)W) xa.state[pos / 64] |= 1ULL << (pos % 64);
       }
     }
@@ -794,17 +773,19 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
     xa.frame_images = d_img;
     xa.frame_signs = d_sgn;
     xa.frame_rows = (u32)frame.rows;
-    pq::DevBufs b = E->bufs();
     ++E->launches;
-    if ((e = pq::launch_expect<W, ALG>(xa, b, E->partials, E->grid, E->stream)) != cudaSuccess)
+    if ((e = pq::launch_expect<W, ALG>(xa, E->keys[E->cur], E->coeffs[E->cur], n_fin, E->partials, E->expect_grid,
+                                       E->stream)) != cudaSuccess)
       return E->cuda_fail(e, "expectation launch");
-    std::vector<pq::ExpectPartial> parts(E->grid);
+    cudaEventRecord(E->ev_end, E->stream);
+    std::vector<pq::ExpectPartial> parts(E->expect_grid);
     cudaMemcpyAsync(parts.data(), E->partials, parts.size() * sizeof(pq::ExpectPartial), cudaMemcpyDeviceToHost,
                     E->stream);
     if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "expectation");
     double hi = 0, lo = 0;
     auto dd = [&](double v) {
-      double s = hi + v, bb = s - hi, er = (hi - (s - bb)) + (v - bb);
+      const double s = hi + v, bb = s - hi;
+      double er = (hi - (s - bb)) + (v - bb);
       er += lo;
       hi = s + er;
       lo = er - (hi - s);
@@ -818,77 +799,68 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
     if (diag) res->expectation_value = hi + lo;
     res->terms_below_cutoff = has_c ? below : 0;
   } else {
-    cudaStreamSynchronize(E->stream);
+    cudaEventRecord(E->ev_end, E->stream);
+    if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "sync");
   }
 
-  // Per-gate live counts.
-  if (n_terms_out) {
+  if (n_terms_out)
     for (size_t gi = 0; gi < n_gates; ++gi) n_terms_out[gi] = gate_op[gi] >= 0 ? hist[gate_op[gi]] : n0;
-  }
-  // Final terms.
+
   E->out_keys.clear();
   E->out_coeffs.clear();
   if (cfg->want_terms && n_fin) {
     E->out_keys.resize(n_fin * W);
     E->out_coeffs.resize(n_fin);
-    pq::DevBufs b = E->bufs();
     if (frame.identity) {
-      cudaMemcpyAsync(E->out_keys.data(), b.keys, n_fin * W * 8, cudaMemcpyDeviceToHost, E->stream);
-      cudaMemcpyAsync(E->out_coeffs.data(), b.coeffs, n_fin * 8, cudaMemcpyDeviceToHost, E->stream);
+      cudaMemcpyAsync(E->out_keys.data(), E->keys[E->cur], n_fin * W * 8, cudaMemcpyDeviceToHost, E->stream);
+      cudaMemcpyAsync(E->out_coeffs.data(), E->coeffs[E->cur], n_fin * 8, cudaMemcpyDeviceToHost, E->stream);
     } else {
-      u64* ok = nullptr;
-      double* oc = nullptr;
-      if ((e = cudaMalloc(&ok, n_fin * W * 8)) != cudaSuccess) return E->cuda_fail(e, "terms");
-      if ((e = cudaMalloc(&oc, n_fin * 8)) != cudaSuccess) {
-        cudaFree(ok);
-        return E->cuda_fail(e, "terms");
-      }
+      // The alternate buffer is free after the sweep: conjugate into it.
+      const int alt = E->cur ^ 1;
       ++E->launches;
-      pq::launch_conjugate<W>(b, d_img, d_sgn, (u32)frame.rows, ALG, ok, oc, n_fin, E->stream);
-      cudaMemcpyAsync(E->out_keys.data(), ok, n_fin * W * 8, cudaMemcpyDeviceToHost, E->stream);
-      cudaMemcpyAsync(E->out_coeffs.data(), oc, n_fin * 8, cudaMemcpyDeviceToHost, E->stream);
-      cudaStreamSynchronize(E->stream);
-      cudaFree(ok);
-      cudaFree(oc);
+      pq::launch_conjugate<W>(E->keys[E->cur], E->coeffs[E->cur], n_fin, d_img, d_sgn, (u32)frame.rows, ALG,
+                              E->keys[alt], E->coeffs[alt], E->stream);
+      cudaMemcpyAsync(E->out_keys.data(), E->keys[alt], n_fin * W * 8, cudaMemcpyDeviceToHost, E->stream);
+      cudaMemcpyAsync(E->out_coeffs.data(), E->coeffs[alt], n_fin * 8, cudaMemcpyDeviceToHost, E->stream);
     }
     if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "terms copy");
   }
-  // Per-kind totals (the algorithmic-bytes roofline inputs).
-  res->gate_ms = res->noise_ms = res->phase_ms = 0;
-  res->gate_ops = res->noise_ops = res->phase_ops = 0;
-  res->sum_rows_gate = res->sum_anti = res->sum_children = res->sum_rows_noise = res->sum_kept = 0;
+
+  // Per-kind totals (inputs of the algorithmic-bytes roofline) and the
+  // device-clock split of the sweep time by op kind.
   for (size_t i = 0; i < ops.size(); ++i) {
     const u64 n_in = i ? hist[i - 1] : n0;
-    float op_ms = 0;
-    if (E->profile) cudaEventElapsedTime(&op_ms, E->op_events[2 * i], E->op_events[2 * i + 1]);
+    const double op_ms = i ? (double)(stamps[i] - stamps[i - 1]) * 1e-6 : 0.0;
     switch (ops[i].kind) {
-      case OP_GATE:
+      case pq::OP_GATE:
         ++res->gate_ops;
         res->gate_ms += op_ms;
         res->sum_rows_gate += n_in;
         res->sum_anti += anti[i];
         res->sum_children += hist[i] - n_in;
         break;
-      case OP_PHASE:
+      case pq::OP_PHASE:
         ++res->phase_ops;
         res->phase_ms += op_ms;
+        res->sum_rows_phase += n_in;
         break;
       default:
         ++res->noise_ops;
         res->noise_ms += op_ms;
         res->sum_rows_noise += n_in;
-        res->sum_kept += hist[i];
+        res->sum_kept += ops[i].kind == pq::OP_NOISE_COMPACT ? hist[i] : 0;
     }
   }
   float ms = 0;
-  cudaEventElapsedTime(&ms, E->ev0, E->ev1);
+  cudaEventElapsedTime(&ms, E->ev_begin, E->ev_end);
   res->device_ms = ms;
+  res->sweep_ms = sweep_ms;
+  res->sweep_launches = sweep_launches;
   res->n_final = n_fin;
-  res->peak_terms = hfin.peak;
+  res->peak_terms = peak;
   res->sparse_key_bytes = n_fin * W * 8 + E->tcap * 8;
   res->n_layers_run = n_layers;
   res->n_gates_run = n_gates;
-  (void)noise_op_of_layer;
   return PQ_OK;
 }
 
@@ -921,15 +893,20 @@ int pq_engine_create(pq_engine** out, int device) {
     return PQ_ERR_CUDA;
   }
   if ((e = cudaSetDevice(device)) != cudaSuccess) return PQ_ERR_CUDA;
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  if (!coop) return PQ_ERR_CUDA;
   E->device = device;
   if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess) return PQ_ERR_CUDA;
-  if (cudaMalloc(&E->ctl, sizeof(pq::Ctl)) != cudaSuccess) return PQ_ERR_OOM;
-  if (cudaMallocHost(&E->h_ctl, sizeof(pq::Ctl)) != cudaSuccess) return PQ_ERR_OOM;
-  E->grid = pq::launch_blocks();
-  if (cudaMalloc(&E->partials, sizeof(pq::ExpectPartial) * E->grid) != cudaSuccess) return PQ_ERR_OOM;
-  cudaEventCreate(&E->ev0);
-  cudaEventCreate(&E->ev1);
-  cudaMemset(E->ctl, 0, sizeof(pq::Ctl));
+  if (cudaMalloc(&E->st, sizeof(pq::SweepState)) != cudaSuccess) return PQ_ERR_OOM;
+  if (cudaMallocHost(&E->h_st, sizeof(pq::SweepState)) != cudaSuccess) return PQ_ERR_OOM;
+  if (cudaMalloc(&E->d_err, sizeof(u32)) != cudaSuccess) return PQ_ERR_OOM;
+  cudaMemset(E->d_err, 0, sizeof(u32));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  E->expect_grid = 4 * sms;
+  if (cudaMalloc(&E->partials, sizeof(pq::ExpectPartial) * E->expect_grid) != cudaSuccess) return PQ_ERR_OOM;
+  for (cudaEvent_t* ev : {&E->ev_begin, &E->ev_end, &E->ev_l0, &E->ev_l1}) cudaEventCreate(ev);
   *out = E.release();
   return PQ_OK;
 }

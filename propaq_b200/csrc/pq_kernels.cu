@@ -1,6 +1,9 @@
 // pq_kernels.cu -- the hot path of the B200 propagation engine.
 //
-// One gate is ONE persistent kernel (gate_kernel).  It replaces the
+// The whole op sequence of a propagation (noise layers and gates, in
+// Heisenberg order) runs as ONE cooperative persistent kernel, sweep_kernel.
+// Its blocks are co-resident; a bounded grid barrier separates consecutive
+// ops, so a gate costs no launch.  Per gate the kernel replaces the
 // reference's scan -> route -> absorb -> claim -> rescue rounds
 // (crates/core/src/engine/partitioned_termsum.rs:276-450,
 //  crates/core/src/engine/termsum.rs:561-800) with a single pass:
@@ -9,22 +12,22 @@
 //   * an anticommuting row looks its child K = G.S up in the open-addressing
 //     hash table (pre-gate rows only).  K -> G.K is an involution, so a row
 //     has at most one partner; the lower row of a pair owns both
-//     coefficients and applies the pair rule to both, reading the pre-gate
+//     coefficients and applies the pair rule to both from the pre-gate
 //     values, so no coefficient is ever written by two threads;
 //   * a lone row whose branch survives the emit cutoff creates its child;
 //     children are appended in row order through a warp-ballot / block scan
 //     and a decoupled look-back across tiles, and inserted into the table by
 //     atomicCAS on the packed (fingerprint, row) slot.
 //
-// Rows are never removed by a gate; a noisy layer's reclaim (noise_kernel)
-// damps, filters and compacts them in row order into the ping-pong buffers
-// and re-inserts the survivors into a cleared table.
+// Rows are never removed by a gate.  A noisy layer damps every row; with a
+// truncation configured it then clears the table, filters the rows, compacts
+// the survivors in row order into the other row buffer and re-inserts them
+// (termsum.rs:472-497).
 //
-// Every kernel uses the same persistent-grid protocol: it reads the live
-// count of the current parity from the device control block at entry, takes
-// tiles from an atomic ticket, and the last block to leave publishes the new
-// count and resets the counters.  All spin-waits are bounded and raise an
-// error bit instead of hanging.
+// Before each gate the kernel checks that twice the live count fits the row
+// capacity (a gate appends at most one child per row).  If it does not, every
+// block stops at that op and the host grows the buffers and relaunches from
+// it.  Every spin-wait is bounded and raises an error bit instead of hanging.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -44,19 +47,49 @@ static_assert(ITEMS * NWARPS == 32, "tile scan uses one warp");
 constexpr u32 ST_AGG = 1u, ST_INC = 2u;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr long LOOKBACK_SPIN_LIMIT = 1L << 22;  // ~0.3 s with the backoff below
+constexpr long BARRIER_SPIN_LIMIT = 1L << 25;   // ~2 s with the backoff below
 
 enum : int { S_EMIT = 0, S_HELD = 1, S_DROP = 2 };
 
 __device__ __forceinline__ u64 pack_status(u32 epoch, u32 flag, u32 value) {
   return ((u64)(epoch & 0x3fffffffu) << 34) | ((u64)flag << 32) | value;
 }
-
 __device__ __forceinline__ u64 ld_volatile(const u64* p) { return *(const volatile u64*)p; }
 __device__ __forceinline__ void st_volatile(u64* p, u64 v) { *(volatile u64*)p = v; }
 
+// Grid barrier (sense by generation).  Every block of the cooperative launch
+// calls it; the wait is bounded and, once expired, raises
+// ERR_BARRIER_TIMEOUT so every later barrier falls straight through.
+__device__ __forceinline__ void grid_barrier(SweepState* st, u32& gen) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const u32 g = gen;
+    const u32 arrived = atomicAdd(&st->bar_count, 1u);
+    if (arrived == gridDim.x - 1) {
+      st->bar_count = 0;
+      __threadfence();
+      atomicExch(&st->bar_gen, g + 1);
+    } else {
+      long spins = 0;
+      while (*(volatile u32*)&st->bar_gen == g) {
+        if (*(volatile u32*)&st->error & ERR_BARRIER_TIMEOUT) break;
+        if (++spins > BARRIER_SPIN_LIMIT) {
+          atomicOr(&st->error, ERR_BARRIER_TIMEOUT);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    gen = g + 1;
+    __threadfence();
+  }
+  __syncthreads();
+}
+
 // Decoupled look-back (called by all lanes of warp 0): publishes this tile's
 // aggregate, walks predecessors 32 at a time, returns the exclusive prefix.
-__device__ u32 lookback(u64* status, u32 tile, u32 agg, u32 epoch, Ctl* ctl) {
+__device__ u32 lookback(u64* status, u32 tile, u32 agg, u32 epoch, SweepState* st) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
     if (lane == 0) st_volatile(&status[0], pack_status(epoch, ST_INC, agg));
@@ -68,26 +101,25 @@ __device__ u32 lookback(u64* status, u32 tile, u32 agg, u32 epoch, Ctl* ctl) {
   long spins = 0;
   const u32 ep = epoch & 0x3fffffffu;
   for (;;) {
-    long idx = base - lane;
+    const long idx = base - lane;
     u32 flag, val;
     if (idx >= 0) {
-      u64 s = ld_volatile(&status[idx]);
-      bool fresh = (u32)(s >> 34) == ep;
-      flag = fresh ? (u32)((s >> 32) & 3u) : 0u;
+      const u64 s = ld_volatile(&status[idx]);
+      flag = ((u32)(s >> 34) == ep) ? (u32)((s >> 32) & 3u) : 0u;
       val = (u32)s;
     } else {
       flag = ST_INC;
       val = 0;
     }
-    unsigned inc = __ballot_sync(FULL, flag == ST_INC);
-    unsigned inv = __ballot_sync(FULL, flag == 0);
-    unsigned need = inc ? ((inc & (0u - inc)) << 1) - 1 : FULL;  // lanes up to the nearest inclusive
+    const unsigned inc = __ballot_sync(FULL, flag == ST_INC);
+    const unsigned inv = __ballot_sync(FULL, flag == 0);
+    const unsigned need = inc ? ((inc & (0u - inc)) << 1) - 1 : FULL;  // lanes up to the nearest inclusive
     if (inv & need) {
       if (++spins > LOOKBACK_SPIN_LIMIT) {
-        if (lane == 0) atomicOr(&ctl->error, ERR_LOOKBACK_TIMEOUT);
+        if (lane == 0) atomicOr(&st->error, ERR_LOOKBACK_TIMEOUT);
         break;
       }
-      __nanosleep(64);
+      __nanosleep(32);
       continue;
     }
     u32 v = ((need >> lane) & 1u) ? val : 0u;
@@ -102,18 +134,18 @@ __device__ u32 lookback(u64* status, u32 tile, u32 agg, u32 epoch, Ctl* ctl) {
 }
 
 template <int W>
-__device__ __forceinline__ void load_key(const u64* __restrict__ keys, u64 row, u64* k) {
+__device__ __forceinline__ void load_key(const u64* keys, u64 row, u64* k) {
   const u64* p = keys + row * W;
   if constexpr (W % 2 == 0) {
 #pragma unroll
     for (int i = 0; i < W; i += 2) {
-      ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p + i));
+      const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(p + i));
       k[i] = v.x;
       k[i + 1] = v.y;
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < W; ++i) k[i] = __ldg(p + i);
+    for (int i = 0; i < W; ++i) k[i] = __ldcg(p + i);
   }
 }
 template <int W>
@@ -128,11 +160,11 @@ __device__ __forceinline__ void store_key(u64* keys, u64 row, const u64* k) {
   }
 }
 
-// Row holding key q among rows < n_pre, or -1.  Rows inserted by the running
-// gate (>= n_pre) are skipped: no lookup of this gate can target them.
+// Row holding key q among rows < n_pre, or -1.  Rows the running gate appends
+// (>= n_pre) are skipped: no lookup of this gate can target them.
 template <int W>
-__device__ long long lookup(const u64* q, u64 n_pre, const u64* __restrict__ keys, const u64* table,
-                            u64 mask, Ctl* ctl) {
+__device__ long long lookup(const u64* q, u64 n_pre, const u64* keys, const u64* table, u64 mask,
+                            SweepState* st) {
   const u64 h = key_hash<W>(q);
   const u32 fp = (u32)(h >> 32);
   u64 i = h & mask;
@@ -144,17 +176,17 @@ __device__ long long lookup(const u64* q, u64 n_pre, const u64* __restrict__ key
       const u64* kp = keys + (u64)row * W;
       bool eq = true;
 #pragma unroll
-      for (int w = 0; w < W; ++w) eq &= __ldg(kp + w) == q[w];
+      for (int w = 0; w < W; ++w) eq &= __ldcg(kp + w) == q[w];
       if (eq) return row;
     }
     i = (i + 1) & mask;
   }
-  atomicOr(&ctl->error, ERR_PROBE_OVERFLOW);
+  atomicOr(&st->error, ERR_PROBE_OVERFLOW);
   return -1;
 }
 
 template <int W>
-__device__ void insert(const u64* q, u64 row, u64* table, u64 mask, Ctl* ctl) {
+__device__ void insert(const u64* q, u64 row, u64* table, u64 mask, u32* error) {
   const u64 h = key_hash<W>(q);
   const u64 v = ((h >> 32) << 32) | (row & 0xffffffffULL);
   u64 i = h & mask;
@@ -162,16 +194,13 @@ __device__ void insert(const u64* q, u64 row, u64* table, u64 mask, Ctl* ctl) {
     if (__ldcg(table + i) == EMPTY_SLOT && atomicCAS(table + i, EMPTY_SLOT, v) == EMPTY_SLOT) return;
     i = (i + 1) & mask;
   }
-  atomicOr(&ctl->error, ERR_PROBE_OVERFLOW);
+  atomicOr(error, ERR_PROBE_OVERFLOW);
 }
 
 // -(Im phase) of G*K = i^p * sign: the sin-branch multiplier (coeff.rs:151-168).
 __device__ __forceinline__ double neg_im(int p, double sign) {
   return p == 1 ? -sign : (p == 3 ? sign : 0.0);
 }
-
-template <class Ops>
-struct OpsOf;
 
 template <int ALG>
 struct Alg;
@@ -184,90 +213,44 @@ struct Alg<1> {
   using T = MajoranaOps;
 };
 
-// Shared-memory block used by every compaction kernel.
 struct TileSmem {
   u32 tile;
   u32 excl;
   u32 cnt[32];  // item-major per-warp counts, then their exclusive prefixes
 };
 
-// Entry: decide (uniformly for the whole grid) whether this op runs.
-__device__ __forceinline__ void op_entry(Ctl* ctl, u64 cap_needed, u64 cap, u32 op, u64* n_out, u32* par_out,
-                                         u32* epoch_out, bool* skip_out) {
-  const u32 par = *(volatile u32*)&ctl->parity;
-  const u64 n = *(volatile u64*)&ctl->n[par];
-  const u32 halt = *(volatile u32*)&ctl->halt;
-  bool skip = halt != NOT_HALTED;
-  if (!skip && cap_needed > cap) {
-    skip = true;
-    if (threadIdx.x == 0) atomicMin(&ctl->halt, op);
-  }
-  *n_out = n;
-  *par_out = par;
-  *epoch_out = *(volatile u32*)&ctl->epoch;
-  *skip_out = skip;
-}
-
-// Exit: the last block out publishes the new count and resets the protocol.
-__device__ __forceinline__ void op_exit(Ctl* ctl, u64* hist, u32 op, bool skip, bool changes_n, u32 par,
-                                        u64 n_in, u32 ntiles, u32 epoch) {
+__device__ __forceinline__ u32 next_tile(u32* ticket, TileSmem& sm) {
+  if (threadIdx.x == 0) sm.tile = atomicAdd(ticket, 1u);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const u32 d = atomicAdd(&ctl->done, 1u);
-    if (d == gridDim.x - 1) {
-      __threadfence();
-      u64 n_new = n_in;
-      if (!skip && changes_n) {
-        n_new = ntiles ? *(volatile u64*)&ctl->n_next : n_in;
-        ctl->n[par ^ 1u] = n_new;
-        ctl->parity = par ^ 1u;
-      }
-      if (!skip) {
-        if (hist) hist[op] = n_new;
-        if (n_new > ctl->peak) ctl->peak = n_new;
-      }
-      ctl->ticket = 0;
-      ctl->done = 0;
-      ctl->epoch = epoch + 1;
-      __threadfence();
-    }
-  }
+  return sm.tile;
 }
 
-__device__ __forceinline__ u32 next_tile(Ctl* ctl, TileSmem& sm) {
-  if (threadIdx.x == 0) sm.tile = atomicAdd(&ctl->ticket, 1u);
-  __syncthreads();
-  const u32 t = sm.tile;
-  return t;
-}
-
-// Item-major block scan of ITEMS emit flags per thread + look-back.
-// Returns the per-item exclusive rank base for this warp in sm.cnt and the
-// tile's global exclusive prefix in sm.excl.
-__device__ __forceinline__ void tile_scan(u32 emit_mask, unsigned* masks, TileSmem& sm, u64* status, u32 t,
-                                          u32 ntiles, u64 n_base, u32 epoch, Ctl* ctl) {
+// Item-major block scan of ITEMS flags per thread, then the look-back.  Leaves
+// each (item, warp) exclusive rank base in sm.cnt and the tile's global
+// exclusive prefix in sm.excl; the last tile publishes the op's new count.
+__device__ __forceinline__ void tile_scan(u32 flags, unsigned* masks, TileSmem& sm, u64* status, u32 t, u32 ntiles,
+                                          u64 n_base, u32 epoch, SweepState* st, u64* n_out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k) {
-    masks[k] = __ballot_sync(FULL, (emit_mask >> k) & 1u);
+    masks[k] = __ballot_sync(FULL, (flags >> k) & 1u);
     if (lane == 0) sm.cnt[k * NWARPS + warp] = __popc(masks[k]);
   }
   __syncthreads();
   if (warp == 0) {
-    u32 v = sm.cnt[lane];
+    const u32 v = sm.cnt[lane];
     u32 inc = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      u32 y = __shfl_up_sync(FULL, inc, o);
+      const u32 y = __shfl_up_sync(FULL, inc, o);
       if (lane >= o) inc += y;
     }
     sm.cnt[lane] = inc - v;
     const u32 agg = __shfl_sync(FULL, inc, 31);
-    const u32 excl = lookback(status, t, agg, epoch, ctl);
+    const u32 excl = lookback(status, t, agg, epoch, st);
     if (lane == 0) {
       sm.excl = excl;
-      if (t == ntiles - 1) *(volatile u64*)&ctl->n_next = n_base + excl + agg;
+      if (t == ntiles - 1) st_volatile(n_out, n_base + excl + agg);
     }
   }
   __syncthreads();
@@ -275,213 +258,254 @@ __device__ __forceinline__ void tile_scan(u32 emit_mask, unsigned* masks, TileSm
 
 // ------------------------------------------------------------------ gate
 template <int W, int ALG>
-__global__ void __launch_bounds__(BLOCK) gate_kernel(const GateArgs<W> a, const DevBufs b) {
+__device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, const u64* keys,
+                                        double* coeffs, TileSmem& sm) {
   using Ops = typename Alg<ALG>::T;
-  __shared__ TileSmem sm;
-  Ctl* ctl = b.ctl;
-  u64 N;
-  u32 par, epoch;
-  bool skip;
-  op_entry(ctl, 0, 0, a.op, &N, &par, &epoch, &skip);
-  // Children this gate can create are at most the anticommuting rows, so
-  // 2N rows must fit before the gate may start.
-  if (!skip && 2 * N > b.cap) {
-    skip = true;
-    if (threadIdx.x == 0) atomicMin(&ctl->halt, a.op);
-  }
+  SweepState* st = a.st;
   const u32 ntiles = (u32)((N + TILE - 1) / TILE);
-  if (!skip) {
-    // TermBudget: below the floor, every lossy predicate is off (termsum.rs:60-76).
-    const bool lossless = a.min_terms && N < a.min_terms;
-    const u32 wcut = lossless ? NO_WEIGHT_CUT : a.max_weight;
-    const bool ccut = !lossless && a.has_min_coeff;
-    const double minc = a.min_coeff;
-    const double sn = a.sn, cs = a.cs;
-    // Emit state of a source with coefficient c, branch b and child key ch
-    // (termsum.rs:701-751): HELD by the magnitude precheck, DROP by weight,
-    // else EMIT.
-    auto state = [&](double c, const u64* ch) -> int {
-      if (ccut && fabs(c * sn) < minc) return S_HELD;
-      if (wcut != NO_WEIGHT_CUT && Ops::template weight<W>(ch, a.n_units) > wcut) return S_DROP;
-      return S_EMIT;
-    };
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    u32 n_anti = 0;
-    for (;;) {
-      const u32 t = next_tile(ctl, sm);
-      if (t >= ntiles) break;
-      u32 emit_mask = 0;
-      double bval[ITEMS];
-#pragma unroll
-      for (int k = 0; k < ITEMS; ++k) {
-        bval[k] = 0.0;
-        const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
-        if (r >= N) continue;
-        u64 key[W];
-        load_key<W>(b.keys, r, key);
-        if (!Ops::template anticommutes<W>(a.g, key)) continue;
-        ++n_anti;
-        u64 q[W];
-#pragma unroll
-        for (int w = 0; w < W; ++w) q[w] = key[w] ^ a.g.gen[w];
-        const long long j = lookup<W>(q, N, b.keys, b.table, b.table_mask, ctl);
-        if (j >= 0 && (u64)j < r) continue;  // the lower row of the pair owns it
-        const double c = b.coeffs[r];
-        const double bi = (c * sn) * neg_im(Ops::template product_exp<W>(a.g, key), a.g.sign);
-        const int si = state(c, q);
-        if (j < 0) {
-          b.coeffs[r] = c * cs;
-          if (si == S_EMIT) {
-            emit_mask |= 1u << k;
-            bval[k] = bi;
-          }
-        } else {
-          const double cj = b.coeffs[j];
-          const double bj = (cj * sn) * neg_im(Ops::template product_exp<W>(a.g, q), a.g.sign);
-          const int sj = state(cj, key);
-          const bool to_j = si == S_EMIT || (si == S_HELD && sj == S_EMIT);
-          const bool to_i = sj == S_EMIT || (sj == S_HELD && si == S_EMIT);
-          double ni = c * cs;
-          if (to_i) ni = ni + bj;
-          double nj = cj * cs;
-          if (to_j) nj = nj + bi;
-          b.coeffs[r] = ni;
-          b.coeffs[j] = nj;
-        }
-      }
-      unsigned masks[ITEMS];
-      tile_scan(emit_mask, masks, sm, b.status, t, ntiles, N, epoch, ctl);
-      const unsigned lt = (1u << lane) - 1u;
-#pragma unroll
-      for (int k = 0; k < ITEMS; ++k) {
-        if (!((emit_mask >> k) & 1u)) continue;
-        const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
-        const u64 row = N + sm.excl + sm.cnt[k * NWARPS + warp] + __popc(masks[k] & lt);
-        if (row >= b.cap) {
-          atomicOr(&ctl->error, ERR_CAPACITY);
-          continue;
-        }
-        u64 q[W];
-        load_key<W>(b.keys, r, q);
-#pragma unroll
-        for (int w = 0; w < W; ++w) q[w] ^= a.g.gen[w];
-        store_key<W>(b.keys, row, q);
-        b.coeffs[row] = bval[k];
-        insert<W>(q, row, b.table, b.table_mask, ctl);
-      }
-      __syncthreads();
-    }
-    // per-op count of anticommuting rows (one atomic per warp)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n_anti += __shfl_xor_sync(FULL, n_anti, o);
-    if (lane == 0 && n_anti && b.anti) atomicAdd(b.anti + a.op, (u64)n_anti);
+  u64* n_out = &st->n[(op + 1) & 1];
+  if (ntiles == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(n_out, N);
+    return;
   }
-  op_exit(ctl, b.hist, a.op, skip, true, par, N, ntiles, epoch);
+  if (blockIdx.x >= ntiles) return;  // more blocks than tiles: the rest wait at the barrier
+  // TermBudget: below the floor every lossy predicate is off (termsum.rs:60-76).
+  const bool lossless = a.min_terms && N < a.min_terms;
+  const u32 wcut = lossless ? NO_WEIGHT_CUT : a.max_weight;
+  const bool ccut = !lossless && a.has_min_coeff;
+  const double minc = a.min_coeff;
+  const double sn = d.sn, cs = d.cs;
+  const GenInfo<W>& g = d.g;
+  const u32 epoch = a.epoch_base + op;
+  // Emit state of a source with coefficient c and child key ch
+  // (termsum.rs:701-751): HELD by the magnitude precheck, DROP by weight, else EMIT.
+  auto state = [&](double c, const u64* ch) -> int {
+    if (ccut && fabs(__dmul_rn(c, sn)) < minc) return S_HELD;
+    if (wcut != NO_WEIGHT_CUT && Ops::template weight<W>(ch, a.n_units) > wcut) return S_DROP;
+    return S_EMIT;
+  };
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  u32 n_anti = 0;
+  for (;;) {
+    const u32 t = next_tile(a.tickets + op, sm);
+    if (t >= ntiles) break;
+    u32 emit = 0;
+    double bval[ITEMS];
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      bval[k] = 0.0;
+      const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
+      if (r >= N) continue;
+      u64 key[W];
+      load_key<W>(keys, r, key);
+      if (!Ops::template anticommutes<W>(g, key)) continue;
+      ++n_anti;
+      u64 q[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w) q[w] = key[w] ^ g.gen[w];
+      const long long j = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+      if (j >= 0 && (u64)j < r) continue;  // the lower row of the pair owns it
+      const double c = __ldcg(coeffs + r);
+      const double bi = __dmul_rn(__dmul_rn(c, sn), neg_im(Ops::template product_exp<W>(g, key), g.sign));
+      const int si = state(c, q);
+      if (j < 0) {
+        coeffs[r] = __dmul_rn(c, cs);
+        if (si == S_EMIT) {
+          emit |= 1u << k;
+          bval[k] = bi;
+        }
+      } else {
+        const double cj = __ldcg(coeffs + j);
+        const double bj = __dmul_rn(__dmul_rn(cj, sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
+        const int sj = state(cj, key);
+        const bool to_j = si == S_EMIT || (si == S_HELD && sj == S_EMIT);
+        const bool to_i = sj == S_EMIT || (sj == S_HELD && si == S_EMIT);
+        double ni = __dmul_rn(c, cs);
+        if (to_i) ni = __dadd_rn(ni, bj);
+        double nj = __dmul_rn(cj, cs);
+        if (to_j) nj = __dadd_rn(nj, bi);
+        coeffs[r] = ni;
+        coeffs[j] = nj;
+      }
+    }
+    unsigned masks[ITEMS];
+    tile_scan(emit, masks, sm, a.status, t, ntiles, N, epoch, st, n_out);
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+      if (!((emit >> k) & 1u)) continue;
+      const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
+      const u64 row = N + sm.excl + sm.cnt[k * NWARPS + warp] + __popc(masks[k] & lt);
+      if (row >= a.cap) {
+        atomicOr(&st->error, ERR_CAPACITY);
+        continue;
+      }
+      u64 q[W];
+      load_key<W>(keys, r, q);
+#pragma unroll
+      for (int w = 0; w < W; ++w) q[w] ^= g.gen[w];
+      store_key<W>(const_cast<u64*>(keys), row, q);
+      coeffs[row] = bval[k];
+      insert<W>(q, row, a.table, a.table_mask, &st->error);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) n_anti += __shfl_xor_sync(FULL, n_anti, o);
+  if (lane == 0 && n_anti && a.anti) atomicAdd(a.anti + op, (u64)n_anti);
 }
 
 // A rotation with |sin| < 1e-9 only scales the anticommuting rows by cos
 // (partitioned_termsum.rs:303-308, termsum.rs:551-557).
 template <int W, int ALG>
-__global__ void __launch_bounds__(BLOCK) phase_only_kernel(const GateArgs<W> a, const DevBufs b) {
+__device__ __forceinline__ void phase_op(const GateDesc<W>& d, u64 N, const u64* keys, double* coeffs) {
   using Ops = typename Alg<ALG>::T;
-  __shared__ TileSmem sm;
-  Ctl* ctl = b.ctl;
-  u64 N;
-  u32 par, epoch;
-  bool skip;
-  op_entry(ctl, 0, 0, a.op, &N, &par, &epoch, &skip);
-  const u32 ntiles = (u32)((N + TILE - 1) / TILE);
-  if (!skip) {
-    for (;;) {
-      const u32 t = next_tile(ctl, sm);
-      if (t >= ntiles) break;
-#pragma unroll
-      for (int k = 0; k < ITEMS; ++k) {
-        const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
-        if (r >= N) continue;
-        u64 key[W];
-        load_key<W>(b.keys, r, key);
-        if (Ops::template anticommutes<W>(a.g, key)) b.coeffs[r] *= a.cs;
-      }
-      __syncthreads();
-    }
+  for (u64 r = (u64)blockIdx.x * BLOCK + threadIdx.x; r < N; r += (u64)gridDim.x * BLOCK) {
+    u64 key[W];
+    load_key<W>(keys, r, key);
+    if (Ops::template anticommutes<W>(d.g, key)) coeffs[r] = __dmul_rn(__ldcg(coeffs + r), d.cs);
   }
-  op_exit(ctl, b.hist, a.op, skip, false, par, N, ntiles, epoch);
 }
 
-// ----------------------------------------------------------------- noise
-// One noisy layer: c *= factor[min(w, len-1)] (engine.rs:119-125), then the
-// reclaim keeps weight <= cut and |c| >= cut (termsum.rs:472-497,
-// partitioned_termsum.rs:581-608), compacting survivors in row order into
-// the alternate buffers and re-inserting them into the (cleared) table.
+// Noise without truncation: c *= factor[min(w, len-1)] (engine.rs:119-125).
 template <int W, int ALG>
-__global__ void __launch_bounds__(BLOCK) noise_kernel(const NoiseArgs a, const DevBufs b) {
+__device__ __forceinline__ void noise_scale_op(const SweepArgs& a, const double* factors, u64 N, const u64* keys,
+                                               double* coeffs) {
   using Ops = typename Alg<ALG>::T;
-  __shared__ TileSmem sm;
-  Ctl* ctl = b.ctl;
-  u64 N;
-  u32 par, epoch;
-  bool skip;
-  op_entry(ctl, 0, 0, a.op, &N, &par, &epoch, &skip);
+  const u32 last = a.table_len - 1;
+  for (u64 r = (u64)blockIdx.x * BLOCK + threadIdx.x; r < N; r += (u64)gridDim.x * BLOCK) {
+    u64 key[W];
+    load_key<W>(keys, r, key);
+    const u32 w = Ops::template weight<W>(key, a.n_units);
+    coeffs[r] = __dmul_rn(__ldcg(coeffs + r), __ldg(factors + (w < last ? w : last)));
+  }
+}
+
+// Noise with truncation: damp, keep weight <= cut and |c| >= cut
+// (partitioned_termsum.rs:581-608), compact survivors in row order into the
+// other buffer and re-insert them into the cleared table.
+template <int W, int ALG>
+__device__ __forceinline__ void noise_compact_op(const SweepArgs& a, const double* factors, u32 op, u64 N,
+                                                 const u64* keys, const double* coeffs, u64* keys_out,
+                                                 double* coeffs_out, TileSmem& sm) {
+  using Ops = typename Alg<ALG>::T;
+  SweepState* st = a.st;
   const u32 ntiles = (u32)((N + TILE - 1) / TILE);
-  if (!skip) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const u32 last = a.table_len - 1;
-    for (;;) {
-      const u32 t = next_tile(ctl, sm);
-      if (t >= ntiles) break;
-      u32 keep_mask = 0;
-      double cv[ITEMS];
+  u64* n_out = &st->n[(op + 1) & 1];
+  if (ntiles == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
+    return;
+  }
+  if (blockIdx.x >= ntiles) return;
+  const u32 last = a.table_len - 1;
+  const u32 epoch = a.epoch_base + op;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    const u32 t = next_tile(a.tickets + op, sm);
+    if (t >= ntiles) break;
+    u32 keep = 0;
+    double cv[ITEMS];
 #pragma unroll
-      for (int k = 0; k < ITEMS; ++k) {
-        cv[k] = 0.0;
-        const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
-        if (r >= N) continue;
-        u64 key[W];
-        load_key<W>(b.keys, r, key);
-        const u32 w = Ops::template weight<W>(key, a.n_units);
-        const double c = b.coeffs[r] * __ldg(a.factors + (w < last ? w : last));
-        if (!a.compact) {
-          b.coeffs[r] = c;
-          continue;
-        }
-        cv[k] = c;
-        const bool keep = (a.max_weight == NO_WEIGHT_CUT || w <= a.max_weight) &&
-                          (!a.has_min_coeff || fabs(c) >= a.min_coeff);
-        keep_mask |= (u32)keep << k;
-      }
-      if (a.compact) {
-        unsigned masks[ITEMS];
-        tile_scan(keep_mask, masks, sm, b.status, t, ntiles, 0, epoch, ctl);
-        const unsigned lt = (1u << lane) - 1u;
+    for (int k = 0; k < ITEMS; ++k) {
+      cv[k] = 0.0;
+      const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
+      if (r >= N) continue;
+      u64 key[W];
+      load_key<W>(keys, r, key);
+      const u32 w = Ops::template weight<W>(key, a.n_units);
+      const double c = __dmul_rn(__ldcg(coeffs + r), __ldg(factors + (w < last ? w : last)));
+      cv[k] = c;
+      const bool kp = (a.max_weight == NO_WEIGHT_CUT || w <= a.max_weight) &&
+                      (!a.has_min_coeff || fabs(c) >= a.min_coeff);
+      keep |= (u32)kp << k;
+    }
+    unsigned masks[ITEMS];
+    tile_scan(keep, masks, sm, a.status, t, ntiles, 0, epoch, st, n_out);
+    const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
-        for (int k = 0; k < ITEMS; ++k) {
-          if (!((keep_mask >> k) & 1u)) continue;
-          const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
-          const u64 row = sm.excl + sm.cnt[k * NWARPS + warp] + __popc(masks[k] & lt);
-          u64 key[W];
-          load_key<W>(b.keys, r, key);
-          store_key<W>(b.keys_alt, row, key);
-          b.coeffs_alt[row] = cv[k];
-          insert<W>(key, row, b.table, b.table_mask, ctl);
-        }
+    for (int k = 0; k < ITEMS; ++k) {
+      if (!((keep >> k) & 1u)) continue;
+      const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
+      const u64 row = sm.excl + sm.cnt[k * NWARPS + warp] + __popc(masks[k] & lt);
+      u64 key[W];
+      load_key<W>(keys, r, key);
+      store_key<W>(keys_out, row, key);
+      coeffs_out[row] = cv[k];
+      insert<W>(key, row, a.table, a.table_mask, &st->error);
+    }
+    __syncthreads();
+  }
+}
+
+template <int W, int ALG>
+__global__ void __launch_bounds__(BLOCK) sweep_kernel(const SweepArgs a) {
+  __shared__ TileSmem sm;
+  __shared__ GateDesc<W> sgate;
+  SweepState* st = a.st;
+  u32 gen = *(volatile u32*)&st->bar_gen;
+  int cur = (int)a.cur0;
+  u32 op = a.op_begin;
+  for (; op < a.op_end; ++op) {
+    const OpDesc od = a.ops[op];
+    const u64 N = ld_volatile(&st->n[op & 1]);
+    const u64* keys = a.keys[cur];
+    double* coeffs = a.coeffs[cur];
+    if (od.kind == OP_GATE || od.kind == OP_PHASE) {
+      if (od.kind == OP_GATE && 2 * N > a.cap) {  // uniform: every block reads the same N
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->halt = op;
+        break;
       }
+      if (threadIdx.x == 0) sgate = reinterpret_cast<const GateDesc<W>*>(a.gates)[od.idx];
       __syncthreads();
+      if (od.kind == OP_GATE) {
+        gate_op<W, ALG>(a, sgate, op, N, keys, coeffs, sm);
+      } else {
+        phase_op<W, ALG>(sgate, N, keys, coeffs);
+        if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
+      }
+    } else if (od.kind == OP_NOISE_SCALE) {
+      noise_scale_op<W, ALG>(a, a.tables + (u64)od.idx * a.table_len, N, keys, coeffs);
+      if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
+    } else {
+      for (u64 i = (u64)blockIdx.x * BLOCK + threadIdx.x; i <= a.table_mask; i += (u64)gridDim.x * BLOCK)
+        a.table[i] = EMPTY_SLOT;
+      grid_barrier(st, gen);
+      noise_compact_op<W, ALG>(a, a.tables + (u64)od.idx * a.table_len, op, N, keys, coeffs, a.keys[cur ^ 1],
+                               a.coeffs[cur ^ 1], sm);
+      cur ^= 1;
+    }
+    grid_barrier(st, gen);
+    if (*(volatile u32*)&st->error) {
+      ++op;
+      break;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      const u64 n_new = ld_volatile(&st->n[(op + 1) & 1]);
+      a.hist[op] = n_new;
+      if (n_new > st->peak) st->peak = n_new;
+      if (a.stamps) {
+        u64 t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        a.stamps[op] = t;
+      }
     }
   }
-  op_exit(ctl, b.hist, a.op, skip, a.compact != 0, par, N, ntiles, epoch);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->cur = (u32)cur;
+    st->end_op = op;
+  }
 }
 
 // ------------------------------------------------------------ expectation
-// Generic phase exponent of gen*key for a raw generator (used by the frame
-// conjugation, where every tableau row acts as a generator).
+// Phase exponent of gen*key for a raw generator (the frame conjugation uses
+// every tableau row as a generator).
 template <int W, int ALG>
 __device__ int product_exp_raw(const u64* gen, const u64* key) {
   if constexpr (ALG == 0) {
     int yg = 0, yk = 0, yo = 0, zx = 0;
 #pragma unroll
     for (int i = 0; i < W; ++i) {
-      u64 o = key[i] ^ gen[i];
+      const u64 o = key[i] ^ gen[i];
       yg += __popcll(gen[i] & (gen[i] >> 1) & EVEN);
       yk += __popcll(key[i] & (key[i] >> 1) & EVEN);
       yo += __popcll(o & (o >> 1) & EVEN);
@@ -490,11 +514,11 @@ __device__ int product_exp_raw(const u64* gen, const u64* key) {
     return (yg + yk - yo + 2 * zx) & 3;
   } else {
     int lg = 0, lk = 0, lo = 0, sw = 0;
-    u32 above = 0;  // parity of gen modes in higher words
+    u32 above = 0;  // parity of generator modes in higher words
 #pragma unroll
     for (int i = W - 1; i >= 0; --i) {
-      u64 o = key[i] ^ gen[i];
-      int pg = __popcll(gen[i]), pk = __popcll(key[i]);
+      const u64 o = key[i] ^ gen[i];
+      const int pg = __popcll(gen[i]), pk = __popcll(key[i]);
       lg += pg;
       lk += pk;
       lo += __popcll(o);
@@ -513,10 +537,9 @@ __device__ int product_exp_raw(const u64* gen, const u64* key) {
   }
 }
 
-// Readout conjugation through a deferred Clifford frame
-// (tableau.rs:93-143): fold the rows selected by the key's bits, tracking the
-// phase of the rebuilt source and of the image; the sign is -1 iff their
-// ratio is -1.
+// Readout conjugation through a deferred Clifford frame (tableau.rs:93-143):
+// fold the rows selected by the key's bits, tracking the phase of the rebuilt
+// source and of the image; the sign is -1 iff their ratio is -1.
 template <int W, int ALG>
 __device__ double conjugate_key(const u64* key, const u64* images, const int* signs, u32 rows, u64* out) {
   u64 src[W];
@@ -538,59 +561,57 @@ __device__ double conjugate_key(const u64* key, const u64* images, const int* si
       se += product_exp_raw<W, ALG>(e, src);
       src[wi] ^= e[wi];
       const u64* img = images + (u64)p * W;
-      u64 g[W];
+      u64 gk[W];
 #pragma unroll
-      for (int i = 0; i < W; ++i) g[i] = __ldg(img + i);
-      ie += product_exp_raw<W, ALG>(g, out) + (signs[p] < 0 ? 2 : 0);
+      for (int i = 0; i < W; ++i) gk[i] = __ldg(img + i);
+      ie += product_exp_raw<W, ALG>(gk, out) + (signs[p] < 0 ? 2 : 0);
 #pragma unroll
-      for (int i = 0; i < W; ++i) out[i] ^= g[i];
+      for (int i = 0; i < W; ++i) out[i] ^= gk[i];
     }
   }
   return (((ie - se) & 3) == 2) ? -1.0 : 1.0;
 }
 
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
-  s = a + b;
-  double bb = s - a;
-  e = (a - (s - bb)) + (b - bb);
+  s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
 }
 __device__ __forceinline__ void dd_add(double& hi, double& lo, double v) {
   double s, e;
   two_sum(hi, v, s, e);
-  e += lo;
+  e = __dadd_rn(e, lo);
   two_sum(s, e, hi, lo);
 }
 
 // sum c * <s|frame(K)|s> in double-double, plus the count of |c| < min_coeff
 // (partitioned_termsum.rs:611-697).
 template <int W, int ALG>
-__global__ void __launch_bounds__(BLOCK) expect_kernel(const ExpectArgs a, const DevBufs b,
-                                                       ExpectPartial* partials) {
+__global__ void __launch_bounds__(BLOCK) expect_kernel(const ExpectArgs a, const u64* keys, const double* coeffs,
+                                                       u64 N, ExpectPartial* partials) {
   using Ops = typename Alg<ALG>::T;
-  const u64 N = b.ctl->n[b.ctl->parity];
   double hi = 0, lo = 0, ab = 0;
   u64 below = 0;
   for (u64 r = (u64)blockIdx.x * BLOCK + threadIdx.x; r < N; r += (u64)gridDim.x * BLOCK) {
     u64 key[W];
-    load_key<W>(b.keys, r, key);
-    const double c = b.coeffs[r];
+    load_key<W>(keys, r, key);
+    const double c = coeffs[r];
     if (a.has_min_coeff && fabs(c) < a.min_coeff) ++below;
     double v;
     if (a.frame_images) {
       u64 img[W];
       const double sg = conjugate_key<W, ALG>(key, a.frame_images, a.frame_signs, a.frame_rows, img);
-      v = c * sg * Ops::template trace<W>(img, a.state, a.n_units);
+      v = __dmul_rn(__dmul_rn(c, sg), Ops::template trace<W>(img, a.state, a.n_units));
     } else {
-      v = c * Ops::template trace<W>(key, a.state, a.n_units);
+      v = __dmul_rn(c, Ops::template trace<W>(key, a.state, a.n_units));
     }
     if (v != 0.0) {
       dd_add(hi, lo, v);
       ab += fabs(v);
     }
   }
-  // warp then block reduction (double-double)
   for (int o = 16; o > 0; o >>= 1) {
-    double ohi = __shfl_xor_sync(FULL, hi, o), olo = __shfl_xor_sync(FULL, lo, o);
+    const double ohi = __shfl_xor_sync(FULL, hi, o), olo = __shfl_xor_sync(FULL, lo, o);
     dd_add(hi, lo, ohi);
     dd_add(hi, lo, olo);
     ab += __shfl_xor_sync(FULL, ab, o);
@@ -619,94 +640,88 @@ __global__ void __launch_bounds__(BLOCK) expect_kernel(const ExpectArgs a, const
   }
 }
 
-// Re-inserts rows [0, N) into a cleared table (after a capacity change).
 template <int W>
-__global__ void rebuild_kernel(const DevBufs b) {
-  const u64 N = b.ctl->n[b.ctl->parity];
+__global__ void rebuild_kernel(const u64* keys, u64 N, u64* table, u64 mask, u32* error) {
   for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (u64)gridDim.x * blockDim.x) {
     u64 key[W];
-    load_key<W>(b.keys, r, key);
-    insert<W>(key, r, b.table, b.table_mask, b.ctl);
+    load_key<W>(keys, r, key);
+    insert<W>(key, r, table, mask, error);
   }
 }
 
-// Final terms through the readout frame, sign folded into the coefficient.
 template <int W, int ALG>
-__global__ void conjugate_kernel(const DevBufs b, const u64* images, const int* signs, u32 rows, u64* out_keys,
-                                 double* out_coeffs, u64 n) {
+__global__ void conjugate_kernel(const u64* keys, const double* coeffs, u64 n, const u64* images, const int* signs,
+                                 u32 rows, u64* out_keys, double* out_coeffs) {
   for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (u64)gridDim.x * blockDim.x) {
     u64 key[W], img[W];
-    load_key<W>(b.keys, r, key);
+    load_key<W>(keys, r, key);
     const double sg = conjugate_key<W, ALG>(key, images, signs, rows, img);
     store_key<W>(out_keys, r, img);
-    out_coeffs[r] = b.coeffs[r] * sg;
+    out_coeffs[r] = __dmul_rn(coeffs[r], sg);
   }
 }
 
 }  // namespace
 
-int launch_blocks() {
+template <int W, int ALG>
+int sweep_grid() {
   static int cached = 0;
   if (cached) return cached;
   int dev = 0, sms = 148, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gate_kernel<4, 0>, BLOCK, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<W, ALG>, BLOCK, 0);
   if (per_sm < 1) per_sm = 1;
   cached = sms * per_sm;
   return cached;
 }
 
 template <int W, int ALG>
-cudaError_t launch_gate(const GateArgs<W>& a, const DevBufs& b, int grid, cudaStream_t s) {
-  gate_kernel<W, ALG><<<grid, BLOCK, 0, s>>>(a, b);
-  return cudaGetLastError();
+cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s) {
+  SweepArgs args = a;
+  void* params[] = {&args};
+  return cudaLaunchCooperativeKernel((const void*)sweep_kernel<W, ALG>, dim3(grid), dim3(BLOCK), params, 0, s);
 }
+
 template <int W, int ALG>
-cudaError_t launch_phase_only(const GateArgs<W>& a, const DevBufs& b, int grid, cudaStream_t s) {
-  phase_only_kernel<W, ALG><<<grid, BLOCK, 0, s>>>(a, b);
-  return cudaGetLastError();
-}
-template <int W, int ALG>
-cudaError_t launch_noise(const NoiseArgs& a, const DevBufs& b, int grid, cudaStream_t s) {
-  noise_kernel<W, ALG><<<grid, BLOCK, 0, s>>>(a, b);
-  return cudaGetLastError();
-}
-template <int W, int ALG>
-cudaError_t launch_expect(const ExpectArgs& a, const DevBufs& b, ExpectPartial* partials, int grid,
-                          cudaStream_t s) {
-  expect_kernel<W, ALG><<<grid, BLOCK, 0, s>>>(a, b, partials);
-  return cudaGetLastError();
-}
-template <int W>
-cudaError_t launch_rebuild(const DevBufs& b, int grid, cudaStream_t s) {
-  rebuild_kernel<W><<<grid, 256, 0, s>>>(b);
-  return cudaGetLastError();
-}
-template <int W>
-cudaError_t launch_conjugate(const DevBufs& b, const u64* images, const int* signs, u32 rows, int alg,
-                             u64* out_keys, double* out_coeffs, u64 n, cudaStream_t s) {
-  const int grid = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
-  if (grid == 0) return cudaSuccess;
-  if (alg == 0)
-    conjugate_kernel<W, 0><<<grid, 256, 0, s>>>(b, images, signs, rows, out_keys, out_coeffs, n);
-  else
-    conjugate_kernel<W, 1><<<grid, 256, 0, s>>>(b, images, signs, rows, out_keys, out_coeffs, n);
+cudaError_t launch_expect(const ExpectArgs& a, const u64* keys, const double* coeffs, u64 n,
+                          ExpectPartial* partials, int grid, cudaStream_t s) {
+  expect_kernel<W, ALG><<<grid, BLOCK, 0, s>>>(a, keys, coeffs, n, partials);
   return cudaGetLastError();
 }
 
-#define PQ_INSTANTIATE(Wv, Av)                                                                         \
-  template cudaError_t launch_gate<Wv, Av>(const GateArgs<Wv>&, const DevBufs&, int, cudaStream_t);       \
-  template cudaError_t launch_phase_only<Wv, Av>(const GateArgs<Wv>&, const DevBufs&, int, cudaStream_t); \
-  template cudaError_t launch_noise<Wv, Av>(const NoiseArgs&, const DevBufs&, int, cudaStream_t);         \
-  template cudaError_t launch_expect<Wv, Av>(const ExpectArgs&, const DevBufs&, ExpectPartial*, int,      \
-                                             cudaStream_t);
+template <int W>
+cudaError_t launch_rebuild(const u64* keys, u64 n, u64* table, u64 mask, u32* error, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const u64 blocks = (n + 255) / 256;
+  rebuild_kernel<W><<<(int)(blocks < 8192 ? blocks : 8192), 256, 0, s>>>(keys, n, table, mask, error);
+  return cudaGetLastError();
+}
+
+template <int W>
+cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const u64* images, const int* signs,
+                             u32 rows, int alg, u64* out_keys, double* out_coeffs, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const u64 blocks = (n + 255) / 256;
+  const int grid = (int)(blocks < 4096 ? blocks : 4096);
+  if (alg == 0)
+    conjugate_kernel<W, 0><<<grid, 256, 0, s>>>(keys, coeffs, n, images, signs, rows, out_keys, out_coeffs);
+  else
+    conjugate_kernel<W, 1><<<grid, 256, 0, s>>>(keys, coeffs, n, images, signs, rows, out_keys, out_coeffs);
+  return cudaGetLastError();
+}
+
+#define PQ_INSTANTIATE(Wv, Av)                                                                          \
+  template int sweep_grid<Wv, Av>();                                                                    \
+  template cudaError_t launch_sweep<Wv, Av>(const SweepArgs&, int, cudaStream_t);                       \
+  template cudaError_t launch_expect<Wv, Av>(const ExpectArgs&, const u64*, const double*, u64,         \
+                                             ExpectPartial*, int, cudaStream_t);
 #define PQ_INSTANTIATE_W(Wv)                                                                            \
   PQ_INSTANTIATE(Wv, 0)                                                                                 \
   PQ_INSTANTIATE(Wv, 1)                                                                                 \
-  template cudaError_t launch_rebuild<Wv>(const DevBufs&, int, cudaStream_t);                           \
-  template cudaError_t launch_conjugate<Wv>(const DevBufs&, const u64*, const int*, u32, int, u64*, double*, \
-                                            u64, cudaStream_t);
+  template cudaError_t launch_rebuild<Wv>(const u64*, u64, u64*, u64, u32*, cudaStream_t);              \
+  template cudaError_t launch_conjugate<Wv>(const u64*, const double*, u64, const u64*, const int*, u32, int, \
+                                            u64*, double*, cudaStream_t);
 
 PQ_INSTANTIATE_W(1)
 PQ_INSTANTIATE_W(2)

@@ -7,47 +7,65 @@
 
 namespace pq {
 
-// Device buffers of one engine, as the kernels see them.
-struct DevBufs {
-  u64* keys;         // current rows, W words each (row-major)
-  double* coeffs;    // current coefficients
-  u64* keys_alt;     // ping-pong target of a reclaim
-  double* coeffs_alt;
-  u64* table;        // open-addressing slots: (fingerprint << 32) | row
-  u64 table_mask;    // slots - 1
-  u64 cap;           // rows each buffer holds
-  u64* status;       // tile look-back status words
-  Ctl* ctl;
-  u64* hist;         // live count after each op
-  u64* anti;         // anticommuting rows seen by each gate op
+// One step of the op sequence a sweep runs.
+enum OpKind : u32 {
+  OP_GATE = 0,           // branch a rotation (pair rule, emit, append, insert)
+  OP_PHASE = 1,          // |sin| < eps: scale the anticommuting rows by cos
+  OP_NOISE_SCALE = 2,    // damp every row by its weight's factor
+  OP_NOISE_COMPACT = 3,  // damp, then reclaim: filter + compact + re-insert
 };
 
-// Per-gate arguments.
+struct OpDesc {
+  u32 kind;
+  u32 idx;  // GATE / PHASE: gate descriptor; NOISE_*: noise table index
+};
+
 template <int W>
-struct GateArgs {
+struct GateDesc {
   GenInfo<W> g;
-  double sn, cs;        // sin(angle), cos(angle) from the host libm
-  u32 max_weight;       // NO_WEIGHT_CUT if none
-  u32 has_min_coeff;
-  double min_coeff;
-  u64 min_terms;        // TermBudget floor, 0 = none
-  u32 n_units;
-  u32 op;               // op index (capacity halts and the per-op history)
+  double sn, cs;  // sin(angle), cos(angle) from the host libm
 };
 
-struct NoiseArgs {
-  const double* factors;  // factor by weight (device)
+// Device-resident state of a sweep, one per engine.
+struct SweepState {
+  u64 n[2];       // live rows: op k reads n[k & 1], writes n[(k + 1) & 1]
+  u64 peak;       // largest live count the sweeps have seen
+  u32 halt;       // op at which a sweep stopped for capacity, or NOT_HALTED
+  u32 error;      // ERR_* bits
+  u32 cur;        // row buffer holding the live rows when the sweep ended
+  u32 end_op;     // first op the sweep did not run
+  u32 bar_count;  // grid barrier arrivals
+  u32 bar_gen;    // grid barrier generation
+};
+
+struct SweepArgs {
+  const OpDesc* ops;
+  const void* gates;       // GateDesc<W>[]
+  const double* tables;    // noise factor tables, table_len entries each
   u32 table_len;
   u32 n_units;
-  u32 max_weight;         // reclaim predicate; NO_WEIGHT_CUT if none
+  u32 op_begin, op_end;    // ops [op_begin, op_end) of the sequence
+  u32 cur0;                // row buffer holding the live rows at entry
+  u32 epoch_base;          // tags this launch's tile statuses
+  u32 max_weight;          // NO_WEIGHT_CUT if none
   u32 has_min_coeff;
   double min_coeff;
-  u32 compact;            // 0: scale only (no truncation configured)
-  u32 op;
+  u64 min_terms;           // TermBudget floor, 0 = none
+  u64* keys[2];            // row keys, W words each, double buffered
+  double* coeffs[2];
+  u64* table;              // open-addressing slots: (fingerprint << 32) | row
+  u64 table_mask;
+  u64 cap;                 // rows each buffer holds
+  u64* status;             // tile look-back status words
+  u32* tickets;            // per-op tile counters, zero at entry
+  u64* hist;               // live count after each op
+  u64* anti;               // anticommuting rows each gate op saw
+  u64* stamps;             // %globaltimer at the end of each op
+  SweepState* st;
 };
 
 struct ExpectArgs {
-  u64 state[64];          // basis state in key layout (Pauli: bit 2q+1; Majorana: bit 2k)
+  u64 state[64];            // basis state in key layout (Pauli: bit 2q+1; Majorana: bit 2k)
   u32 n_units;
   u32 has_min_coeff;
   double min_coeff;
@@ -57,27 +75,25 @@ struct ExpectArgs {
 };
 
 struct ExpectPartial {
-  double hi, lo;      // double-double partial sum of c * trace
-  double abs_sum;     // sum of |c * trace|
-  u64 below;          // |c| < min_coeff
+  double hi, lo;    // double-double partial sum of c * trace
+  double abs_sum;   // sum of |c * trace|
+  u64 below;        // |c| < min_coeff
 };
 
-int launch_blocks();  // persistent grid size for the current device
+// Largest co-resident grid of the sweep kernel for this W / algebra.
+template <int W, int ALG>
+int sweep_grid();
 
 template <int W, int ALG>
-cudaError_t launch_gate(const GateArgs<W>& a, const DevBufs& b, int grid, cudaStream_t s);
+cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s);
 template <int W, int ALG>
-cudaError_t launch_phase_only(const GateArgs<W>& a, const DevBufs& b, int grid, cudaStream_t s);
-template <int W, int ALG>
-cudaError_t launch_noise(const NoiseArgs& a, const DevBufs& b, int grid, cudaStream_t s);
-template <int W, int ALG>
-cudaError_t launch_expect(const ExpectArgs& a, const DevBufs& b, ExpectPartial* partials, int grid,
-                          cudaStream_t s);
+cudaError_t launch_expect(const ExpectArgs& a, const u64* keys, const double* coeffs, u64 n,
+                          ExpectPartial* partials, int grid, cudaStream_t s);
 template <int W>
-cudaError_t launch_rebuild(const DevBufs& b, int grid, cudaStream_t s);
+cudaError_t launch_rebuild(const u64* keys, u64 n, u64* table, u64 table_mask, u32* error, cudaStream_t s);
 template <int W>
-cudaError_t launch_conjugate(const DevBufs& b, const u64* frame_images, const int* frame_signs,
-                             u32 frame_rows, int alg, u64* out_keys, double* out_coeffs, u64 n,
-                             cudaStream_t s);
+cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const u64* frame_images,
+                             const int* frame_signs, u32 frame_rows, int alg, u64* out_keys,
+                             double* out_coeffs, cudaStream_t s);
 
 }  // namespace pq
