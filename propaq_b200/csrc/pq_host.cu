@@ -41,7 +41,7 @@ namespace {
 constexpr double EPS_CLASSIFY = 1e-9;  // termsum.rs:42, partitioned_termsum.rs:41
 constexpr u32 MAX_UNITS = 2048;        // engine.rs:27
 constexpr u64 MAX_ROWS = 1ULL << 31;   // row index ceiling of the table slots
-constexpr int TILE_ROWS = 1024;
+constexpr int TILE_ROWS = 256;  // smallest tile a sweep uses (sizes the look-back status array)
 
 inline int hpopc(u64 x) { return __builtin_popcountll(x); }
 constexpr u64 EVEN = 0x5555555555555555ULL;
@@ -323,7 +323,6 @@ struct pq_engine {
   // per-op device arrays
   size_t ops_cap = 0;
   pq::OpDesc* d_ops = nullptr;
-  u32* tickets = nullptr;
   u64* hist = nullptr;
   u64* anti = nullptr;
   u64* stamps = nullptr;
@@ -361,10 +360,9 @@ struct pq_engine {
     cap = tcap = 0;
   }
   void free_ops() {
-    for (void* p : {(void*)d_ops, (void*)tickets, (void*)hist, (void*)anti, (void*)stamps})
+    for (void* p : {(void*)d_ops, (void*)hist, (void*)anti, (void*)stamps})
       if (p) cudaFree(p);
     d_ops = nullptr;
-    tickets = nullptr;
     hist = anti = stamps = nullptr;
     ops_cap = 0;
   }
@@ -448,7 +446,7 @@ struct pq_engine {
     free_ops();
     cudaError_t e;
     if ((e = cudaMalloc(&d_ops, n_ops * sizeof(pq::OpDesc))) != cudaSuccess ||
-        (e = cudaMalloc(&tickets, n_ops * 4)) != cudaSuccess || (e = cudaMalloc(&hist, n_ops * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&hist, n_ops * 8)) != cudaSuccess ||
         (e = cudaMalloc(&anti, n_ops * 8)) != cudaSuccess || (e = cudaMalloc(&stamps, n_ops * 8)) != cudaSuccess)
       return cuda_fail(e, "allocating op arrays");
     ops_cap = n_ops;
@@ -600,6 +598,7 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
   const int grid = pq::sweep_grid<W, ALG>();
   double sweep_ms = 0;
   u64 sweep_launches = 0;
+  bool began = false;
 
   // Runs ops [done, ops.size()) on the device; on a capacity halt grows the
   // rows and relaunches from the halted op.
@@ -621,7 +620,6 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
       s.bar_gen = 0;
       *E->h_st = s;
       cudaMemcpyAsync(E->st, E->h_st, sizeof s, cudaMemcpyHostToDevice, E->stream);
-      cudaMemsetAsync(E->tickets + done, 0, (ops.size() - done) * 4, E->stream);
       pq::SweepArgs a{};
       a.ops = E->d_ops;
       a.gates = E->d_gates;
@@ -644,11 +642,14 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
       a.table_mask = E->tcap - 1;
       a.cap = E->cap;
       a.status = E->status;
-      a.tickets = E->tickets;
       a.hist = E->hist;
       a.anti = E->anti;
       a.stamps = E->stamps;
       a.st = E->st;
+      if (!began) {  // device time starts at the first sweep
+        cudaEventRecord(E->ev_begin, E->stream);
+        began = true;
+      }
       cudaEventRecord(E->ev_l0, E->stream);
       if ((e = pq::launch_sweep<W, ALG>(a, grid, E->stream)) != cudaSuccess) return E->cuda_fail(e, "sweep launch");
       cudaEventRecord(E->ev_l1, E->stream);
@@ -684,7 +685,6 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
     return PQ_OK;
   };
 
-  cudaEventRecord(E->ev_begin, E->stream);
   Tableau frame(ALG, W, n_units);
   std::vector<u64> g(W), gc(W);
   long last_op = -1;
@@ -728,6 +728,7 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
     }
   }
   if (int rc = flush()) return rc;
+  if (!began) cudaEventRecord(E->ev_begin, E->stream);
   const u64 n_fin = n_live;
 
   std::vector<u64> hist(ops.size()), anti(ops.size()), stamps(ops.size());

@@ -40,9 +40,14 @@ namespace {
 
 constexpr int BLOCK = 256;
 constexpr int NWARPS = BLOCK / 32;
-constexpr int ITEMS = 4;  // rows per thread per tile; ITEMS * NWARPS == 32
-constexpr int TILE = BLOCK * ITEMS;
-static_assert(ITEMS * NWARPS == 32, "tile scan uses one warp");
+constexpr int MAX_ITEMS = 4;  // rows per thread per tile; items * NWARPS <= 32
+static_assert(MAX_ITEMS * NWARPS <= 32, "tile scan uses one warp");
+// Rows per thread for a gate over many rows: enough independent loads in
+// flight per thread without spilling the keys kept in registers.
+template <int W>
+struct Items {
+  static constexpr int value = W <= 2 ? 2 : 1;
+};
 
 constexpr u32 ST_AGG = 1u, ST_INC = 2u;
 constexpr unsigned FULL = 0xffffffffu;
@@ -160,14 +165,17 @@ __device__ __forceinline__ void store_key(u64* keys, u64 row, const u64* k) {
   }
 }
 
-// Row holding key q among rows < n_pre, or -1.  Rows the running gate appends
-// (>= n_pre) are skipped: no lookup of this gate can target them.
+// The table is linear-probed from a bucket of 4 slots (one 32-byte sector):
+// a lookup starts at the first slot of the key's bucket and scans forward
+// until it meets the key or an empty slot; an insert takes the first empty
+// slot of the same sequence.
+__device__ __forceinline__ u64 bucket_start(u64 h, u64 mask) { return (h & mask) & ~3ULL; }
+
+// Continues a lookup of q from slot i (see bucket_start).  Rows the running
+// gate appends (>= n_pre) are skipped: no lookup of this gate can target them.
 template <int W>
-__device__ long long lookup(const u64* q, u64 n_pre, const u64* keys, const u64* table, u64 mask,
-                            SweepState* st) {
-  const u64 h = key_hash<W>(q);
-  const u32 fp = (u32)(h >> 32);
-  u64 i = h & mask;
+__device__ long long lookup_from(const u64* q, u32 fp, u64 i, u64 n_pre, const u64* keys, const u64* table,
+                                 u64 mask, SweepState* st) {
   for (u64 probe = 0; probe <= mask; ++probe) {
     const u64 s = __ldcg(table + i);
     if (s == EMPTY_SLOT) return -1;
@@ -189,12 +197,85 @@ template <int W>
 __device__ void insert(const u64* q, u64 row, u64* table, u64 mask, u32* error) {
   const u64 h = key_hash<W>(q);
   const u64 v = ((h >> 32) << 32) | (row & 0xffffffffULL);
-  u64 i = h & mask;
+  u64 i = bucket_start(h, mask);
   for (u64 probe = 0; probe <= mask; ++probe) {
     if (__ldcg(table + i) == EMPTY_SLOT && atomicCAS(table + i, EMPTY_SLOT, v) == EMPTY_SLOT) return;
     i = (i + 1) & mask;
   }
   atomicOr(error, ERR_PROBE_OVERFLOW);
+}
+
+// Looks up the children q[k] = key[k] ^ gen of the items flagged in `want`,
+// with every item's first bucket and candidate key in flight together.
+template <int W, int IT>
+__device__ __forceinline__ void lookup_batch(const u64 (&key)[IT][W], const u64* gen, u32 want, u64 n_pre,
+                                             const u64* keys, const u64* table, u64 mask, SweepState* st,
+                                             long long (&j)[IT]) {
+  u64 h[IT];
+  ulonglong2 b0[IT], b1[IT];
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    j[k] = -1;
+    if (!((want >> k) & 1u)) continue;
+    u64 q[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ gen[w];
+    h[k] = key_hash<W>(q);
+    const ulonglong2* bp = reinterpret_cast<const ulonglong2*>(table + bucket_start(h[k], mask));
+    b0[k] = __ldcg(bp);
+    b1[k] = __ldcg(bp + 1);
+  }
+  // First candidate (fingerprint match among pre-gate rows) before the first
+  // empty slot of the bucket; state: 0 absent, 1 candidate, 2 bucket full.
+  int cand[IT], state[IT];
+  u32 cand_row[IT];
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    state[k] = 0;
+    cand[k] = -1;
+    cand_row[k] = 0;
+    if (!((want >> k) & 1u)) continue;
+    const u64 sl[4] = {b0[k].x, b0[k].y, b1[k].x, b1[k].y};
+    const u32 fp = (u32)(h[k] >> 32);
+    int st2 = 2;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (st2 != 2) continue;
+      if (sl[m] == EMPTY_SLOT) {
+        st2 = 0;
+      } else if ((u32)(sl[m] >> 32) == fp && (u32)sl[m] < n_pre) {
+        st2 = 1;
+        cand[k] = m;
+        cand_row[k] = (u32)sl[m];
+      }
+    }
+    state[k] = st2;
+  }
+  u64 ck[IT][W];
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    if (state[k] != 1) continue;
+    const u64* kp = keys + (u64)cand_row[k] * W;
+#pragma unroll
+    for (int w = 0; w < W; ++w) ck[k][w] = __ldcg(kp + w);
+  }
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    if (!((want >> k) & 1u) || state[k] == 0) continue;
+    u64 q[W];
+    bool eq = state[k] == 1;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      q[w] = key[k][w] ^ gen[w];
+      if (state[k] == 1) eq &= ck[k][w] == q[w];
+    }
+    if (eq) {
+      j[k] = cand_row[k];
+    } else {  // rare: a fingerprint collision or a full bucket, continue in order
+      const u64 next = (bucket_start(h[k], mask) + (state[k] == 1 ? (u64)cand[k] + 1 : 4)) & mask;
+      j[k] = lookup_from<W>(q, (u32)(h[k] >> 32), next, n_pre, keys, table, mask, st);
+    }
+  }
 }
 
 // -(Im phase) of G*K = i^p * sign: the sin-branch multiplier (coeff.rs:151-168).
@@ -214,38 +295,32 @@ struct Alg<1> {
 };
 
 struct TileSmem {
-  u32 tile;
   u32 excl;
   u32 cnt[32];  // item-major per-warp counts, then their exclusive prefixes
 };
 
-__device__ __forceinline__ u32 next_tile(u32* ticket, TileSmem& sm) {
-  if (threadIdx.x == 0) sm.tile = atomicAdd(ticket, 1u);
-  __syncthreads();
-  return sm.tile;
-}
-
-// Item-major block scan of ITEMS flags per thread, then the look-back.  Leaves
+// Item-major block scan of IT flags per thread, then the look-back.  Leaves
 // each (item, warp) exclusive rank base in sm.cnt and the tile's global
 // exclusive prefix in sm.excl; the last tile publishes the op's new count.
+template <int IT>
 __device__ __forceinline__ void tile_scan(u32 flags, unsigned* masks, TileSmem& sm, u64* status, u32 t, u32 ntiles,
                                           u64 n_base, u32 epoch, SweepState* st, u64* n_out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < ITEMS; ++k) {
+  for (int k = 0; k < IT; ++k) {
     masks[k] = __ballot_sync(FULL, (flags >> k) & 1u);
     if (lane == 0) sm.cnt[k * NWARPS + warp] = __popc(masks[k]);
   }
   __syncthreads();
   if (warp == 0) {
-    const u32 v = sm.cnt[lane];
+    const u32 v = lane < IT * NWARPS ? sm.cnt[lane] : 0u;
     u32 inc = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const u32 y = __shfl_up_sync(FULL, inc, o);
       if (lane >= o) inc += y;
     }
-    sm.cnt[lane] = inc - v;
+    if (lane < IT * NWARPS) sm.cnt[lane] = inc - v;
     const u32 agg = __shfl_sync(FULL, inc, 31);
     const u32 excl = lookback(status, t, agg, epoch, st);
     if (lane == 0) {
@@ -257,18 +332,17 @@ __device__ __forceinline__ void tile_scan(u32 flags, unsigned* masks, TileSmem& 
 }
 
 // ------------------------------------------------------------------ gate
-template <int W, int ALG>
-__device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, const u64* keys,
-                                        double* coeffs, TileSmem& sm) {
+// Tiles are assigned statically (tile t to block t mod grid, in order); the
+// cooperative launch keeps every block resident, so a tile's look-back always
+// waits on blocks that are running.
+template <int W, int ALG, int IT>
+__device__ __forceinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
+                                           double* coeffs, TileSmem& sm) {
   using Ops = typename Alg<ALG>::T;
+  constexpr int TL = BLOCK * IT;
   SweepState* st = a.st;
-  const u32 ntiles = (u32)((N + TILE - 1) / TILE);
+  const u32 ntiles = (u32)((N + TL - 1) / TL);
   u64* n_out = &st->n[(op + 1) & 1];
-  if (ntiles == 0) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(n_out, N);
-    return;
-  }
-  if (blockIdx.x >= ntiles) return;  // more blocks than tiles: the rest wait at the barrier
   // TermBudget: below the floor every lossy predicate is off (termsum.rs:60-76).
   const bool lossless = a.min_terms && N < a.min_terms;
   const u32 wcut = lossless ? NO_WEIGHT_CUT : a.max_weight;
@@ -286,73 +360,101 @@ __device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d
   };
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u32 n_anti = 0;
-  for (;;) {
-    const u32 t = next_tile(a.tickets + op, sm);
-    if (t >= ntiles) break;
-    u32 emit = 0;
-    double bval[ITEMS];
+  for (u32 t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    u64 key[IT][W];
+    u32 anti = 0;
 #pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
+    for (int k = 0; k < IT; ++k) {
+      const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
+      if (r < N) load_key<W>(keys, r, key[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
+      if (r < N && Ops::template anticommutes<W>(g, key[k])) anti |= 1u << k;
+    }
+    n_anti += __popc(anti);
+    long long j[IT];
+    lookup_batch<W, IT>(key, g.gen, anti, N, keys, a.table, a.table_mask, st, j);
+    // The lower row of a pair owns both coefficients.
+    u32 own = 0;
+    double c[IT], cj[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
+      if (!((anti >> k) & 1u) || (j[k] >= 0 && (u64)j[k] < r)) continue;
+      own |= 1u << k;
+      c[k] = __ldcg(coeffs + r);
+      cj[k] = j[k] >= 0 ? __ldcg(coeffs + j[k]) : 0.0;
+    }
+    u32 emit = 0;
+    double bval[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
       bval[k] = 0.0;
-      const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
-      if (r >= N) continue;
-      u64 key[W];
-      load_key<W>(keys, r, key);
-      if (!Ops::template anticommutes<W>(g, key)) continue;
-      ++n_anti;
+      if (!((own >> k) & 1u)) continue;
+      const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
       u64 q[W];
 #pragma unroll
-      for (int w = 0; w < W; ++w) q[w] = key[w] ^ g.gen[w];
-      const long long j = lookup<W>(q, N, keys, a.table, a.table_mask, st);
-      if (j >= 0 && (u64)j < r) continue;  // the lower row of the pair owns it
-      const double c = __ldcg(coeffs + r);
-      const double bi = __dmul_rn(__dmul_rn(c, sn), neg_im(Ops::template product_exp<W>(g, key), g.sign));
-      const int si = state(c, q);
-      if (j < 0) {
-        coeffs[r] = __dmul_rn(c, cs);
+      for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ g.gen[w];
+      const double bi = __dmul_rn(__dmul_rn(c[k], sn), neg_im(Ops::template product_exp<W>(g, key[k]), g.sign));
+      const int si = state(c[k], q);
+      if (j[k] < 0) {
+        coeffs[r] = __dmul_rn(c[k], cs);
         if (si == S_EMIT) {
           emit |= 1u << k;
           bval[k] = bi;
         }
       } else {
-        const double cj = __ldcg(coeffs + j);
-        const double bj = __dmul_rn(__dmul_rn(cj, sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
-        const int sj = state(cj, key);
+        const double bj = __dmul_rn(__dmul_rn(cj[k], sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
+        const int sj = state(cj[k], key[k]);
         const bool to_j = si == S_EMIT || (si == S_HELD && sj == S_EMIT);
         const bool to_i = sj == S_EMIT || (sj == S_HELD && si == S_EMIT);
-        double ni = __dmul_rn(c, cs);
+        double ni = __dmul_rn(c[k], cs);
         if (to_i) ni = __dadd_rn(ni, bj);
-        double nj = __dmul_rn(cj, cs);
+        double nj = __dmul_rn(cj[k], cs);
         if (to_j) nj = __dadd_rn(nj, bi);
         coeffs[r] = ni;
-        coeffs[j] = nj;
+        coeffs[j[k]] = nj;
       }
     }
-    unsigned masks[ITEMS];
-    tile_scan(emit, masks, sm, a.status, t, ntiles, N, epoch, st, n_out);
+    unsigned masks[IT];
+    tile_scan<IT>(emit, masks, sm, a.status, t, ntiles, N, epoch, st, n_out);
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
+    for (int k = 0; k < IT; ++k) {
       if (!((emit >> k) & 1u)) continue;
-      const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
       const u64 row = N + sm.excl + sm.cnt[k * NWARPS + warp] + __popc(masks[k] & lt);
       if (row >= a.cap) {
         atomicOr(&st->error, ERR_CAPACITY);
         continue;
       }
       u64 q[W];
-      load_key<W>(keys, r, q);
 #pragma unroll
-      for (int w = 0; w < W; ++w) q[w] ^= g.gen[w];
-      store_key<W>(const_cast<u64*>(keys), row, q);
+      for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ g.gen[w];
+      store_key<W>(keys, row, q);
       coeffs[row] = bval[k];
       insert<W>(q, row, a.table, a.table_mask, &st->error);
     }
-    __syncthreads();
+    __syncthreads();  // sm is reused by the next tile
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) n_anti += __shfl_xor_sync(FULL, n_anti, o);
   if (lane == 0 && n_anti && a.anti) atomicAdd(a.anti + op, (u64)n_anti);
+}
+
+template <int W, int ALG>
+__device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
+                                        double* coeffs, TileSmem& sm) {
+  if (N == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(&a.st->n[(op + 1) & 1], 0);
+    return;
+  }
+  // Few rows: one per thread keeps every row's chain of dependent loads short.
+  if (N <= (u64)gridDim.x * BLOCK)
+    gate_tiles<W, ALG, 1>(a, d, op, N, keys, coeffs, sm);
+  else
+    gate_tiles<W, ALG, Items<W>::value>(a, d, op, N, keys, coeffs, sm);
 }
 
 // A rotation with |sin| < 1e-9 only scales the anticommuting rows by cos
@@ -389,56 +491,58 @@ __device__ __forceinline__ void noise_compact_op(const SweepArgs& a, const doubl
                                                  const u64* keys, const double* coeffs, u64* keys_out,
                                                  double* coeffs_out, TileSmem& sm) {
   using Ops = typename Alg<ALG>::T;
+  constexpr int IT = MAX_ITEMS;
+  constexpr int TL = BLOCK * IT;
   SweepState* st = a.st;
-  const u32 ntiles = (u32)((N + TILE - 1) / TILE);
+  const u32 ntiles = (u32)((N + TL - 1) / TL);
   u64* n_out = &st->n[(op + 1) & 1];
   if (ntiles == 0) {
     if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
     return;
   }
-  if (blockIdx.x >= ntiles) return;
   const u32 last = a.table_len - 1;
   const u32 epoch = a.epoch_base + op;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (;;) {
-    const u32 t = next_tile(a.tickets + op, sm);
-    if (t >= ntiles) break;
+  for (u32 t = blockIdx.x; t < ntiles; t += gridDim.x) {
     u32 keep = 0;
-    double cv[ITEMS];
+    double cv[IT];
+    u64 key[IT][W];
 #pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-      cv[k] = 0.0;
-      const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
+    for (int k = 0; k < IT; ++k) {
+      const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
+      if (r < N) {
+        load_key<W>(keys, r, key[k]);
+        cv[k] = __ldcg(coeffs + r);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
       if (r >= N) continue;
-      u64 key[W];
-      load_key<W>(keys, r, key);
-      const u32 w = Ops::template weight<W>(key, a.n_units);
-      const double c = __dmul_rn(__ldcg(coeffs + r), __ldg(factors + (w < last ? w : last)));
+      const u32 w = Ops::template weight<W>(key[k], a.n_units);
+      const double c = __dmul_rn(cv[k], __ldg(factors + (w < last ? w : last)));
       cv[k] = c;
       const bool kp = (a.max_weight == NO_WEIGHT_CUT || w <= a.max_weight) &&
                       (!a.has_min_coeff || fabs(c) >= a.min_coeff);
       keep |= (u32)kp << k;
     }
-    unsigned masks[ITEMS];
-    tile_scan(keep, masks, sm, a.status, t, ntiles, 0, epoch, st, n_out);
+    unsigned masks[IT];
+    tile_scan<IT>(keep, masks, sm, a.status, t, ntiles, 0, epoch, st, n_out);
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
+    for (int k = 0; k < IT; ++k) {
       if (!((keep >> k) & 1u)) continue;
-      const u64 r = (u64)t * TILE + (u64)k * BLOCK + threadIdx.x;
       const u64 row = sm.excl + sm.cnt[k * NWARPS + warp] + __popc(masks[k] & lt);
-      u64 key[W];
-      load_key<W>(keys, r, key);
-      store_key<W>(keys_out, row, key);
+      store_key<W>(keys_out, row, key[k]);
       coeffs_out[row] = cv[k];
-      insert<W>(key, row, a.table, a.table_mask, &st->error);
+      insert<W>(key[k], row, a.table, a.table_mask, &st->error);
     }
     __syncthreads();
   }
 }
 
 template <int W, int ALG>
-__global__ void __launch_bounds__(BLOCK) sweep_kernel(const SweepArgs a) {
+__global__ void __launch_bounds__(BLOCK, (W >= 8 ? 1 : 2)) sweep_kernel(const SweepArgs a) {
   __shared__ TileSmem sm;
   __shared__ GateDesc<W> sgate;
   SweepState* st = a.st;
@@ -448,7 +552,7 @@ __global__ void __launch_bounds__(BLOCK) sweep_kernel(const SweepArgs a) {
   for (; op < a.op_end; ++op) {
     const OpDesc od = a.ops[op];
     const u64 N = ld_volatile(&st->n[op & 1]);
-    const u64* keys = a.keys[cur];
+    u64* keys = a.keys[cur];
     double* coeffs = a.coeffs[cur];
     if (od.kind == OP_GATE || od.kind == OP_PHASE) {
       if (od.kind == OP_GATE && 2 * N > a.cap) {  // uniform: every block reads the same N

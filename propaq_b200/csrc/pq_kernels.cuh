@@ -57,7 +57,6 @@ struct SweepArgs {
   u64 table_mask;
   u64 cap;                 // rows each buffer holds
   u64* status;             // tile look-back status words
-  u32* tickets;            // per-op tile counters, zero at entry
   u64* hist;               // live count after each op
   u64* anti;               // anticommuting rows each gate op saw
   u64* stamps;             // %globaltimer at the end of each op
