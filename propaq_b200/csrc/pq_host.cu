@@ -213,6 +213,23 @@ struct Tableau {
     t.refresh_identity();
     return t;
   }
+  // changes_weight of for_rotation(gen) without building the tableau: a
+  // single-bit row keeps its image unless it anticommutes with gen, and then
+  // its image is gen ^ e_p.
+  static bool rotation_changes_weight(int alg, int W, u32 n_units, const u64* gen) {
+    const size_t lim = std::min((size_t)2 * n_units, (size_t)64 * W);
+    u64 e[64] = {0}, img[64];
+    for (size_t p = 0; p < lim; ++p) {
+      e[p / 64] = 1ULL << (p % 64);
+      const bool anti = host_anticommutes(alg, W, gen, e);
+      e[p / 64] = 0;
+      if (!anti) continue;
+      for (int i = 0; i < W; ++i) img[i] = gen[i];
+      img[p / 64] ^= 1ULL << (p % 64);
+      if (host_support(W, img) != 1) return true;
+    }
+    return false;
+  }
   bool changes_weight() const {
     for (size_t p = 0; p < rows; ++p) {
       std::vector<u64> u(W, 0);
@@ -700,15 +717,14 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
       std::memcpy(g.data(), gate_words + (size_t)gi * W, 8 * W);
       const double ang = angles[gi];
       if (std::fabs(std::cos(ang)) < EPS_CLASSIFY) {  // Clifford: defer into the frame when allowed
-        Tableau step = Tableau::for_rotation(ALG, W, n_units, g.data(), ang);
         bool eff_w = has_w;
-        const bool cw = step.changes_weight();
+        const bool cw = Tableau::rotation_changes_weight(ALG, W, n_units, g.data());
         if (has_w && cw && has_floor) {  // the effective cutoff depends on the live count here
           if (int rc = flush()) return rc;
           if (n_live < floor_terms) eff_w = false;
         }
         if (!eff_w || !cw) {
-          frame.compose(step);
+          frame.compose(Tableau::for_rotation(ALG, W, n_units, g.data(), ang));
           gate_op[gi] = last_op;
           continue;
         }

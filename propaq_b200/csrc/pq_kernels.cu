@@ -42,12 +42,6 @@ constexpr int BLOCK = 256;
 constexpr int NWARPS = BLOCK / 32;
 constexpr int MAX_ITEMS = 4;  // rows per thread per tile; items * NWARPS <= 32
 static_assert(MAX_ITEMS * NWARPS <= 32, "tile scan uses one warp");
-// Rows per thread for a gate over many rows: enough independent loads in
-// flight per thread without spilling the keys kept in registers.
-template <int W>
-struct Items {
-  static constexpr int value = W <= 2 ? 2 : 1;
-};
 
 constexpr u32 ST_AGG = 1u, ST_INC = 2u;
 constexpr unsigned FULL = 0xffffffffu;
@@ -205,77 +199,31 @@ __device__ void insert(const u64* q, u64 row, u64* table, u64 mask, u32* error) 
   atomicOr(error, ERR_PROBE_OVERFLOW);
 }
 
-// Looks up the children q[k] = key[k] ^ gen of the items flagged in `want`,
-// with every item's first bucket and candidate key in flight together.
-template <int W, int IT>
-__device__ __forceinline__ void lookup_batch(const u64 (&key)[IT][W], const u64* gen, u32 want, u64 n_pre,
-                                             const u64* keys, const u64* table, u64 mask, SweepState* st,
-                                             long long (&j)[IT]) {
-  u64 h[IT];
-  ulonglong2 b0[IT], b1[IT];
+// Row holding q among the pre-gate rows, or -1: the key's first bucket is
+// one 32-byte load, so most lookups finish with it (plus the candidate row's
+// key on a fingerprint match).
+template <int W>
+__device__ __forceinline__ long long lookup(const u64* q, u64 n_pre, const u64* keys, const u64* table, u64 mask,
+                                            SweepState* st) {
+  const u64 h = key_hash<W>(q);
+  const u32 fp = (u32)(h >> 32);
+  const u64 b = bucket_start(h, mask);
+  const ulonglong2* bp = reinterpret_cast<const ulonglong2*>(table + b);
+  const ulonglong2 s01 = __ldcg(bp), s23 = __ldcg(bp + 1);
+  const u64 sl[4] = {s01.x, s01.y, s23.x, s23.y};
 #pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    j[k] = -1;
-    if (!((want >> k) & 1u)) continue;
-    u64 q[W];
+  for (int m = 0; m < 4; ++m) {
+    if (sl[m] == EMPTY_SLOT) return -1;
+    const u32 row = (u32)sl[m];
+    if ((u32)(sl[m] >> 32) == fp && row < n_pre) {
+      const u64* kp = keys + (u64)row * W;
+      bool eq = true;
 #pragma unroll
-    for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ gen[w];
-    h[k] = key_hash<W>(q);
-    const ulonglong2* bp = reinterpret_cast<const ulonglong2*>(table + bucket_start(h[k], mask));
-    b0[k] = __ldcg(bp);
-    b1[k] = __ldcg(bp + 1);
-  }
-  // First candidate (fingerprint match among pre-gate rows) before the first
-  // empty slot of the bucket; state: 0 absent, 1 candidate, 2 bucket full.
-  int cand[IT], state[IT];
-  u32 cand_row[IT];
-#pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    state[k] = 0;
-    cand[k] = -1;
-    cand_row[k] = 0;
-    if (!((want >> k) & 1u)) continue;
-    const u64 sl[4] = {b0[k].x, b0[k].y, b1[k].x, b1[k].y};
-    const u32 fp = (u32)(h[k] >> 32);
-    int st2 = 2;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      if (st2 != 2) continue;
-      if (sl[m] == EMPTY_SLOT) {
-        st2 = 0;
-      } else if ((u32)(sl[m] >> 32) == fp && (u32)sl[m] < n_pre) {
-        st2 = 1;
-        cand[k] = m;
-        cand_row[k] = (u32)sl[m];
-      }
-    }
-    state[k] = st2;
-  }
-  u64 ck[IT][W];
-#pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    if (state[k] != 1) continue;
-    const u64* kp = keys + (u64)cand_row[k] * W;
-#pragma unroll
-    for (int w = 0; w < W; ++w) ck[k][w] = __ldcg(kp + w);
-  }
-#pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    if (!((want >> k) & 1u) || state[k] == 0) continue;
-    u64 q[W];
-    bool eq = state[k] == 1;
-#pragma unroll
-    for (int w = 0; w < W; ++w) {
-      q[w] = key[k][w] ^ gen[w];
-      if (state[k] == 1) eq &= ck[k][w] == q[w];
-    }
-    if (eq) {
-      j[k] = cand_row[k];
-    } else {  // rare: a fingerprint collision or a full bucket, continue in order
-      const u64 next = (bucket_start(h[k], mask) + (state[k] == 1 ? (u64)cand[k] + 1 : 4)) & mask;
-      j[k] = lookup_from<W>(q, (u32)(h[k] >> 32), next, n_pre, keys, table, mask, st);
+      for (int w = 0; w < W; ++w) eq &= __ldcg(kp + w) == q[w];
+      if (eq) return row;
     }
   }
+  return lookup_from<W>(q, fp, (b + 4) & mask, n_pre, keys, table, mask, st);
 }
 
 // -(Im phase) of G*K = i^p * sign: the sin-branch multiplier (coeff.rs:151-168).
@@ -375,7 +323,15 @@ __device__ __forceinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>
     }
     n_anti += __popc(anti);
     long long j[IT];
-    lookup_batch<W, IT>(key, g.gen, anti, N, keys, a.table, a.table_mask, st, j);
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      j[k] = -1;
+      if (!((anti >> k) & 1u)) continue;
+      u64 q[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ g.gen[w];
+      j[k] = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+    }
     // The lower row of a pair owns both coefficients.
     u32 own = 0;
     double c[IT], cj[IT];
@@ -450,11 +406,9 @@ __device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d
     if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(&a.st->n[(op + 1) & 1], 0);
     return;
   }
-  // Few rows: one per thread keeps every row's chain of dependent loads short.
-  if (N <= (u64)gridDim.x * BLOCK)
-    gate_tiles<W, ALG, 1>(a, d, op, N, keys, coeffs, sm);
-  else
-    gate_tiles<W, ALG, Items<W>::value>(a, d, op, N, keys, coeffs, sm);
+  // One row per thread: every row's chain of dependent loads stays short and
+  // the resident warps keep many independent chains in flight.
+  gate_tiles<W, ALG, 1>(a, d, op, N, keys, coeffs, sm);
 }
 
 // A rotation with |sin| < 1e-9 only scales the anticommuting rows by cos
@@ -491,7 +445,7 @@ __device__ __forceinline__ void noise_compact_op(const SweepArgs& a, const doubl
                                                  const u64* keys, const double* coeffs, u64* keys_out,
                                                  double* coeffs_out, TileSmem& sm) {
   using Ops = typename Alg<ALG>::T;
-  constexpr int IT = MAX_ITEMS;
+  constexpr int IT = 1;
   constexpr int TL = BLOCK * IT;
   SweepState* st = a.st;
   const u32 ntiles = (u32)((N + TL - 1) / TL);
@@ -542,7 +496,7 @@ __device__ __forceinline__ void noise_compact_op(const SweepArgs& a, const doubl
 }
 
 template <int W, int ALG>
-__global__ void __launch_bounds__(BLOCK, (W >= 8 ? 1 : 2)) sweep_kernel(const SweepArgs a) {
+__global__ void __launch_bounds__(BLOCK, (W >= 8 ? 2 : (W == 4 ? 3 : 4))) sweep_kernel(const SweepArgs a) {
   __shared__ TileSmem sm;
   __shared__ GateDesc<W> sgate;
   SweepState* st = a.st;

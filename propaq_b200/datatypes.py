@@ -353,15 +353,10 @@ class _TermSum:
 
     def to_arrays(self, n_words: int):
         """(keys [n, n_words] u64, coeffs [n] f64) in insertion order."""
-        n = len(self._terms)
-        keys = np.zeros((n, n_words), dtype=np.uint64)
-        coeffs = np.zeros(n, dtype=np.float64)
-        mask = (1 << 64) - 1
-        for i, (t, c) in enumerate(self._terms.items()):
-            k = t.key()
-            for w in range(n_words):
-                keys[i, w] = (k >> (64 * w)) & mask
-            coeffs[i] = c
+        nb = 8 * n_words
+        buf = b"".join(t.key().to_bytes(nb, "little") for t in self._terms)
+        keys = np.frombuffer(buf, dtype="<u8").reshape(len(self._terms), n_words).astype(np.uint64)
+        coeffs = np.fromiter(self._terms.values(), dtype=np.float64, count=len(self._terms))
         return keys, coeffs
 
 

@@ -53,12 +53,14 @@ def heisenberg_gates(circuit, n_words: int, key_of):
             gens.append(key_of(rot.generator))
             angles.append(float(rot.angle))
         offsets.append(len(angles))
-    g = np.zeros((len(gens), n_words), dtype=np.uint64)
-    mask = (1 << 64) - 1
-    for i, k in enumerate(gens):
-        for w in range(n_words):
-            g[i, w] = (k >> (64 * w)) & mask
-    return g, np.array(angles, dtype=np.float64), np.array(offsets, dtype=np.uint32)
+    return keys_to_words(gens, n_words), np.array(angles, dtype=np.float64), np.array(offsets, dtype=np.uint32)
+
+
+def keys_to_words(keys, n_words: int) -> np.ndarray:
+    """Python-int keys -> [len, n_words] little-endian u64 words."""
+    nb = 8 * n_words
+    buf = b"".join(k.to_bytes(nb, "little") for k in keys)
+    return np.frombuffer(buf, dtype="<u8").reshape(len(keys), n_words).astype(np.uint64)
 
 
 def state_words(initial_state, n_units: int) -> np.ndarray:
