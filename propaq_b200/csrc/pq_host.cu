@@ -340,6 +340,7 @@ struct pq_engine {
   // per-op device arrays
   size_t ops_cap = 0;
   pq::OpDesc* d_ops = nullptr;
+  u32* tickets = nullptr;
   u64* hist = nullptr;
   u64* anti = nullptr;
   u64* stamps = nullptr;
@@ -377,9 +378,10 @@ struct pq_engine {
     cap = tcap = 0;
   }
   void free_ops() {
-    for (void* p : {(void*)d_ops, (void*)hist, (void*)anti, (void*)stamps})
+    for (void* p : {(void*)d_ops, (void*)tickets, (void*)hist, (void*)anti, (void*)stamps})
       if (p) cudaFree(p);
     d_ops = nullptr;
+    tickets = nullptr;
     hist = anti = stamps = nullptr;
     ops_cap = 0;
   }
@@ -463,7 +465,7 @@ struct pq_engine {
     free_ops();
     cudaError_t e;
     if ((e = cudaMalloc(&d_ops, n_ops * sizeof(pq::OpDesc))) != cudaSuccess ||
-        (e = cudaMalloc(&hist, n_ops * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&tickets, n_ops * 4)) != cudaSuccess || (e = cudaMalloc(&hist, n_ops * 8)) != cudaSuccess ||
         (e = cudaMalloc(&anti, n_ops * 8)) != cudaSuccess || (e = cudaMalloc(&stamps, n_ops * 8)) != cudaSuccess)
       return cuda_fail(e, "allocating op arrays");
     ops_cap = n_ops;
@@ -637,6 +639,7 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
       s.bar_gen = 0;
       *E->h_st = s;
       cudaMemcpyAsync(E->st, E->h_st, sizeof s, cudaMemcpyHostToDevice, E->stream);
+      cudaMemsetAsync(E->tickets + done, 0, (ops.size() - done) * 4, E->stream);
       pq::SweepArgs a{};
       a.ops = E->d_ops;
       a.gates = E->d_gates;
@@ -659,6 +662,7 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
       a.table_mask = E->tcap - 1;
       a.cap = E->cap;
       a.status = E->status;
+      a.tickets = E->tickets;
       a.hist = E->hist;
       a.anti = E->anti;
       a.stamps = E->stamps;

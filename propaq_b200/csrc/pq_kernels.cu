@@ -47,6 +47,8 @@ constexpr u32 ST_AGG = 1u, ST_INC = 2u;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr long LOOKBACK_SPIN_LIMIT = 1L << 22;  // ~0.3 s with the backoff below
 constexpr long BARRIER_SPIN_LIMIT = 1L << 25;   // ~2 s with the backoff below
+constexpr u32 BAR_GROUPS = SweepState::BAR_GROUPS;
+constexpr int TILE_LARGE = BLOCK * MAX_ITEMS;
 
 enum : int { S_EMIT = 0, S_HELD = 1, S_DROP = 2 };
 
@@ -56,16 +58,26 @@ __device__ __forceinline__ u64 pack_status(u32 epoch, u32 flag, u32 value) {
 __device__ __forceinline__ u64 ld_volatile(const u64* p) { return *(const volatile u64*)p; }
 __device__ __forceinline__ void st_volatile(u64* p, u64 v) { *(volatile u64*)p = v; }
 
-// Grid barrier (sense by generation).  Every block of the cooperative launch
-// calls it; the wait is bounded and, once expired, raises
-// ERR_BARRIER_TIMEOUT so every later barrier falls straight through.
+// Grid barrier (sense by generation), two-level: each block arrives on one of
+// BAR_GROUPS counters (each on its own 128-byte line), the last arrival of a
+// group arrives on the top counter, and the last top arrival releases
+// everyone by bumping the generation.  Every wait is bounded; once one
+// expires, ERR_BARRIER_TIMEOUT makes every later barrier fall through.
 __device__ __forceinline__ void grid_barrier(SweepState* st, u32& gen) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const u32 g = gen;
-    const u32 arrived = atomicAdd(&st->bar_count, 1u);
-    if (arrived == gridDim.x - 1) {
+    const u32 nb = gridDim.x;
+    const u32 grp = blockIdx.x % BAR_GROUPS;
+    const u32 in_grp = nb / BAR_GROUPS + (grp < nb % BAR_GROUPS ? 1u : 0u);
+    const u32 n_grp = nb < BAR_GROUPS ? nb : BAR_GROUPS;
+    bool last = false;
+    if (atomicAdd(&st->bar_group[grp].count, 1u) == in_grp - 1) {
+      st->bar_group[grp].count = 0;
+      last = atomicAdd(&st->bar_count, 1u) == n_grp - 1;
+    }
+    if (last) {
       st->bar_count = 0;
       __threadfence();
       atomicExch(&st->bar_gen, g + 1);
@@ -77,7 +89,7 @@ __device__ __forceinline__ void grid_barrier(SweepState* st, u32& gen) {
           atomicOr(&st->error, ERR_BARRIER_TIMEOUT);
           break;
         }
-        __nanosleep(32);
+        __nanosleep(20);
       }
     }
     gen = g + 1;
@@ -243,6 +255,7 @@ struct Alg<1> {
 };
 
 struct TileSmem {
+  u32 tile;
   u32 excl;
   u32 cnt[32];  // item-major per-warp counts, then their exclusive prefixes
 };
@@ -284,7 +297,7 @@ __device__ __forceinline__ void tile_scan(u32 flags, unsigned* masks, TileSmem& 
 // cooperative launch keeps every block resident, so a tile's look-back always
 // waits on blocks that are running.
 template <int W, int ALG, int IT>
-__device__ __forceinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
+__device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
                                            double* coeffs, TileSmem& sm) {
   using Ops = typename Alg<ALG>::T;
   constexpr int TL = BLOCK * IT;
@@ -399,6 +412,102 @@ __device__ __forceinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>
   if (lane == 0 && n_anti && a.anti) atomicAdd(a.anti + op, (u64)n_anti);
 }
 
+// Many rows: 1024-row tiles handed out in order by a per-op ticket, each
+// thread taking its MAX_ITEMS rows one after the other.
+template <int W, int ALG>
+__device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
+                                                 double* coeffs, TileSmem& sm) {
+  using Ops = typename Alg<ALG>::T;
+  constexpr int IT = MAX_ITEMS;
+  constexpr int TL = BLOCK * IT;
+  SweepState* st = a.st;
+  const u32 ntiles = (u32)((N + TL - 1) / TL);
+  u64* n_out = &st->n[(op + 1) & 1];
+  const bool lossless = a.min_terms && N < a.min_terms;
+  const u32 wcut = lossless ? NO_WEIGHT_CUT : a.max_weight;
+  const bool ccut = !lossless && a.has_min_coeff;
+  const double minc = a.min_coeff;
+  const double sn = d.sn, cs = d.cs;
+  const GenInfo<W>& g = d.g;
+  const u32 epoch = a.epoch_base + op;
+  auto state = [&](double c, const u64* ch) -> int {
+    if (ccut && fabs(__dmul_rn(c, sn)) < minc) return S_HELD;
+    if (wcut != NO_WEIGHT_CUT && Ops::template weight<W>(ch, a.n_units) > wcut) return S_DROP;
+    return S_EMIT;
+  };
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  u32 n_anti = 0;
+  for (;;) {
+    if (threadIdx.x == 0) sm.tile = atomicAdd(a.tickets + op, 1u);
+    __syncthreads();
+    const u32 t = sm.tile;
+    if (t >= ntiles) break;
+    u32 emit = 0;
+    double bval[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      bval[k] = 0.0;
+      const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
+      if (r >= N) continue;
+      u64 key[W];
+      load_key<W>(keys, r, key);
+      if (!Ops::template anticommutes<W>(g, key)) continue;
+      ++n_anti;
+      u64 q[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w) q[w] = key[w] ^ g.gen[w];
+      const long long j = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+      if (j >= 0 && (u64)j < r) continue;  // the lower row of the pair owns it
+      const double c = __ldcg(coeffs + r);
+      const double bi = __dmul_rn(__dmul_rn(c, sn), neg_im(Ops::template product_exp<W>(g, key), g.sign));
+      const int si = state(c, q);
+      if (j < 0) {
+        coeffs[r] = __dmul_rn(c, cs);
+        if (si == S_EMIT) {
+          emit |= 1u << k;
+          bval[k] = bi;
+        }
+      } else {
+        const double cj = __ldcg(coeffs + j);
+        const double bj = __dmul_rn(__dmul_rn(cj, sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
+        const int sj = state(cj, key);
+        const bool to_j = si == S_EMIT || (si == S_HELD && sj == S_EMIT);
+        const bool to_i = sj == S_EMIT || (sj == S_HELD && si == S_EMIT);
+        double ni = __dmul_rn(c, cs);
+        if (to_i) ni = __dadd_rn(ni, bj);
+        double nj = __dmul_rn(cj, cs);
+        if (to_j) nj = __dadd_rn(nj, bi);
+        coeffs[r] = ni;
+        coeffs[j] = nj;
+      }
+    }
+    unsigned masks[IT];
+    tile_scan<IT>(emit, masks, sm, a.status, t, ntiles, N, epoch, st, n_out);
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      if (!((emit >> k) & 1u)) continue;
+      const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
+      const u64 row = N + sm.excl + sm.cnt[k * NWARPS + warp] + __popc(masks[k] & lt);
+      if (row >= a.cap) {
+        atomicOr(&st->error, ERR_CAPACITY);
+        continue;
+      }
+      u64 q[W];
+      load_key<W>(keys, r, q);
+#pragma unroll
+      for (int w = 0; w < W; ++w) q[w] ^= g.gen[w];
+      store_key<W>(keys, row, q);
+      coeffs[row] = bval[k];
+      insert<W>(q, row, a.table, a.table_mask, &st->error);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) n_anti += __shfl_xor_sync(FULL, n_anti, o);
+  if (lane == 0 && n_anti && a.anti) atomicAdd(a.anti + op, (u64)n_anti);
+}
+
 template <int W, int ALG>
 __device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
                                         double* coeffs, TileSmem& sm) {
@@ -406,15 +515,18 @@ __device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d
     if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(&a.st->n[(op + 1) & 1], 0);
     return;
   }
-  // One row per thread: every row's chain of dependent loads stays short and
-  // the resident warps keep many independent chains in flight.
-  gate_tiles<W, ALG, 1>(a, d, op, N, keys, coeffs, sm);
+  // Few rows: one row per thread and at most one 256-row tile per block, so
+  // every row's chain of dependent loads runs at once.
+  if (N <= (u64)gridDim.x * BLOCK)
+    gate_tiles<W, ALG, 1>(a, d, op, N, keys, coeffs, sm);
+  else
+    gate_tiles_large<W, ALG>(a, d, op, N, keys, coeffs, sm);
 }
 
 // A rotation with |sin| < 1e-9 only scales the anticommuting rows by cos
 // (partitioned_termsum.rs:303-308, termsum.rs:551-557).
 template <int W, int ALG>
-__device__ __forceinline__ void phase_op(const GateDesc<W>& d, u64 N, const u64* keys, double* coeffs) {
+__device__ __noinline__ void phase_op(const GateDesc<W>& d, u64 N, const u64* keys, double* coeffs) {
   using Ops = typename Alg<ALG>::T;
   for (u64 r = (u64)blockIdx.x * BLOCK + threadIdx.x; r < N; r += (u64)gridDim.x * BLOCK) {
     u64 key[W];
@@ -425,7 +537,7 @@ __device__ __forceinline__ void phase_op(const GateDesc<W>& d, u64 N, const u64*
 
 // Noise without truncation: c *= factor[min(w, len-1)] (engine.rs:119-125).
 template <int W, int ALG>
-__device__ __forceinline__ void noise_scale_op(const SweepArgs& a, const double* factors, u64 N, const u64* keys,
+__device__ __noinline__ void noise_scale_op(const SweepArgs& a, const double* factors, u64 N, const u64* keys,
                                                double* coeffs) {
   using Ops = typename Alg<ALG>::T;
   const u32 last = a.table_len - 1;
@@ -441,7 +553,7 @@ __device__ __forceinline__ void noise_scale_op(const SweepArgs& a, const double*
 // (partitioned_termsum.rs:581-608), compact survivors in row order into the
 // other buffer and re-insert them into the cleared table.
 template <int W, int ALG>
-__device__ __forceinline__ void noise_compact_op(const SweepArgs& a, const double* factors, u32 op, u64 N,
+__device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* factors, u32 op, u64 N,
                                                  const u64* keys, const double* coeffs, u64* keys_out,
                                                  double* coeffs_out, TileSmem& sm) {
   using Ops = typename Alg<ALG>::T;

@@ -34,8 +34,12 @@ struct SweepState {
   u32 error;      // ERR_* bits
   u32 cur;        // row buffer holding the live rows when the sweep ended
   u32 end_op;     // first op the sweep did not run
-  u32 bar_count;  // grid barrier arrivals
+  u32 bar_count;  // grid barrier: groups arrived
   u32 bar_gen;    // grid barrier generation
+  static constexpr unsigned BAR_GROUPS = 16;
+  struct alignas(128) Group {
+    u32 count;    // blocks of this group arrived
+  } bar_group[BAR_GROUPS];
 };
 
 struct SweepArgs {
@@ -57,6 +61,7 @@ struct SweepArgs {
   u64 table_mask;
   u64 cap;                 // rows each buffer holds
   u64* status;             // tile look-back status words
+  u32* tickets;            // per-op tile counters for many-row gates, zero at entry
   u64* hist;               // live count after each op
   u64* anti;               // anticommuting rows each gate op saw
   u64* stamps;             // %globaltimer at the end of each op
