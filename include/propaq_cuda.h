@@ -163,6 +163,30 @@ int pq_plugin_truncator_keep(const pq_plugin* plugin, uint32_t basis_kind, const
                              size_t n_words, uint32_t n_units, uint32_t weight,
                              double coeff_magnitude, uint32_t layer_index, uint32_t n_layers);
 
+/* Expectation value sum_i c_i <s|K_i|s> of a term sum held in HOST memory,
+ * for callers that may not allocate device memory.  This entry point has no
+ * counterpart in the reference.
+ *
+ * Who needs it: programs that own all device memory themselves -- frameworks
+ * that reserve (almost) the whole GPU up front for their own allocators, or
+ * applications with a fixed device-memory budget -- where a cudaMalloc from
+ * inside the library fails or breaks the owner's accounting.  It allocates
+ * nothing: the terms are staged into a static __device__ array of
+ * PQ_NOALLOC_SCRATCH_BYTES, which every GPU that loads it holds until the
+ * process exits.  n_terms * (8 * n_words + 8) bytes (plus 8.25 KiB of partial
+ * sums) must fit; larger inputs are refused with PQ_ERR_INVALID and a message
+ * in `err`.  n_units <= 256.
+ *
+ * The first call on a device resolves the array's address on that device
+ * (the current device); make that first call before any stream capture.
+ * Every call shares the array: calls that overlap on one device race, so
+ * serialise them.  Runs on the legacy default stream and returns when the
+ * value has been copied to *out_value. */
+#define PQ_NOALLOC_SCRATCH_BYTES (16u << 20)
+int pq_expectation_noalloc(uint32_t basis_kind, uint32_t n_units, const uint64_t* keys,
+                           const double* coeffs, size_t n_terms, const uint64_t* diag_state,
+                           size_t diag_words, double* out_value, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

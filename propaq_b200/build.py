@@ -19,7 +19,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libpropaq_cuda.so"
-SOURCES = ["pq_kernels.cu", "pq_host.cu"]
+SOURCES = ["pq_kernels.cu", "pq_host.cu", "pq_noalloc.cu"]
 HEADERS = ["pq_device.cuh", "pq_kernels.cuh"]
 
 NVCC_FLAGS = [
