@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "majorana", "majorana_small", "tfim"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="sweep blocks per SM (0 = as many as fit)")
     return ap.parse_args()
 
 
@@ -265,6 +266,7 @@ def main():
         table = np.ascontiguousarray(prob.noise_table, dtype=np.float64)
         cfg.noise_kind, cfg.noise_tables, cfg.noise_table_len = _native.PQ_NOISE_TABLE, table.ctypes.data, len(table)
     cfg.want_terms = 0
+    cfg.blocks_per_sm = args.blocks_per_sm
 
     def device_step():
         return engine.run(cfg, prob.obs_keys, prob.obs_coeffs, prob.gate_keys, prob.angles, prob.offsets, prob.diag)

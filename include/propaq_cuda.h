@@ -81,6 +81,7 @@ typedef struct pq_run_config {
   size_t noise_table_len;    /* entries per table (normally n_units + 1)       */
   const pq_plugin* noise_plugin; /* PLUGIN kind                                 */
   uint32_t want_terms;       /* keep the final terms for pq_result_terms        */
+  uint32_t blocks_per_sm;    /* sweep blocks per SM; 0 = as many as fit (tuning) */
 } pq_run_config;
 
 /* crates/core/src/interface/results.rs:8-51 (PropagationResult), plus the

@@ -49,6 +49,7 @@ class RunConfig(ctypes.Structure):
         ("noise_table_len", ctypes.c_size_t),
         ("noise_plugin", ctypes.c_void_p),
         ("want_terms", ctypes.c_uint32),
+        ("blocks_per_sm", ctypes.c_uint32),
     ]
 
 

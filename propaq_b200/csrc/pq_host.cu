@@ -614,7 +614,7 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
   u64 n_live = n0, peak = n0;
   size_t done = 0;  // ops executed so far
   size_t gdone = 0; // gate descriptors uploaded so far
-  const int grid = pq::sweep_grid<W, ALG>();
+  const int grid = pq::sweep_grid<W, ALG>((int)cfg->blocks_per_sm);
   double sweep_ms = 0;
   u64 sweep_launches = 0;
   bool began = false;

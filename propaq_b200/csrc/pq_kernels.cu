@@ -834,16 +834,17 @@ __global__ void conjugate_kernel(const u64* keys, const double* coeffs, u64 n, c
 }  // namespace
 
 template <int W, int ALG>
-int sweep_grid() {
-  static int cached = 0;
-  if (cached) return cached;
-  int dev = 0, sms = 148, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<W, ALG>, BLOCK, 0);
-  if (per_sm < 1) per_sm = 1;
-  cached = sms * per_sm;
-  return cached;
+int sweep_grid(int blocks_per_sm) {
+  static int sms = 0, per_sm = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<W, ALG>, BLOCK, 0);
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int b = (blocks_per_sm > 0 && blocks_per_sm < per_sm) ? blocks_per_sm : per_sm;
+  return sms * b;
 }
 
 template <int W, int ALG>
@@ -882,7 +883,7 @@ cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const
 }
 
 #define PQ_INSTANTIATE(Wv, Av)                                                                          \
-  template int sweep_grid<Wv, Av>();                                                                    \
+  template int sweep_grid<Wv, Av>(int);                                                                    \
   template cudaError_t launch_sweep<Wv, Av>(const SweepArgs&, int, cudaStream_t);                       \
   template cudaError_t launch_expect<Wv, Av>(const ExpectArgs&, const u64*, const double*, u64,         \
                                              ExpectPartial*, int, cudaStream_t);

@@ -84,9 +84,10 @@ struct ExpectPartial {
   u64 below;        // |c| < min_coeff
 };
 
-// Largest co-resident grid of the sweep kernel for this W / algebra.
+// Co-resident grid of the sweep kernel for this W / algebra: every SM with
+// blocks_per_sm blocks (0 or more than fit = as many as fit).
 template <int W, int ALG>
-int sweep_grid();
+int sweep_grid(int blocks_per_sm);
 
 template <int W, int ALG>
 cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s);
