@@ -17,6 +17,11 @@ coefficient cutoff 1e-5, FP64 coefficients.
              rows, E children); per noisy layer (8W+16)(N + kept); per
              phase-only gate 8W N.
 
+`--workload batch` runs the extrapolation-sweep batch instead: 64 independent
+kicked-Ising instances of 40..100 qubits (4 noise scales x 4 coefficient
+cutoffs x 4 observable sites) in shared persistent launches (pq_run_batch),
+beside the same 64 instances as sequential pq_run calls on the same GPU.
+
 `--impl reference` times the CPU restatement of the reference engine (the
 oracle) on the host cores instead.  With torchrun (N > 1) every rank runs an
 independent replica of the workload (the path does not shard).
@@ -47,10 +52,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "majorana", "majorana_small", "tfim"])
+    ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "majorana", "majorana_small", "tfim", "batch"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="sweep blocks per SM (0 = as many as fit)")
+    ap.add_argument("--split", type=int, default=1, help="batch: 0 equal grid shares, 1 by remaining work")
+    ap.add_argument("--rebalance-pct", type=int, default=25, help="batch: re-split when this %% of the grid idles")
+    ap.add_argument("--no-sequential", action="store_true", help="batch: skip the sequential pq_run comparison")
     return ap.parse_args()
 
 
@@ -194,9 +202,173 @@ def run_cpu_baseline(problem_builder, seconds, cores):
     return terms / el, runs, el, r
 
 
+def main_batch(args, world, rank, local):
+    """The extrapolation-sweep batch: value = term-gate visits of all 64
+    instances per second of the batched launches' device time."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from harness import from_workload, make_cfg, run_oracle
+
+    from propaq_b200 import workloads
+
+    wls = workloads.kicked_ising_batch(64, seed=0)
+    probs = [from_workload(w) for w in wls]
+    cores = os.cpu_count() or 1
+    desc = ("64 kicked-Ising instances, n ~ U{40..100} on the most-square open grid, steps ~ U{8..20}, "
+            "RX theta ~ U[0.2,1.0], grid p in {0.5,1,1.5,2}e-3 x |c| cut in {1e-3..1e-6} x 4 Z sites, w<=10")
+    base_line = {"metric": "terms/s", "unit": "terms/s", "n_gpus": args.gpus, "steps": args.steps,
+                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                 "dtype": "f64", "data": "synthetic (seeded; no dataset)",
+                 "config": {"workload": desc, "name": "kicked_ising_batch64_seed0", "instances": len(probs),
+                            "gates": int(sum(len(p.angles) for p in probs)),
+                            "parallelism": f"replicas x{world}", "l2": "flushed between steps"}}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        o = oracle_load()
+        # A bounded sample: the instances in order until cpu_seconds pass, per step.
+        steps_t, terms_total, inst = [], 0, 0
+        for i in range(args.warmup + args.steps):
+            t0, terms, k = time.perf_counter(), 0, 0
+            while k == 0 or time.perf_counter() - t0 < args.cpu_seconds / max(1, args.warmup + args.steps):
+                r = run_oracle(o, probs[(i + k) % len(probs)], n_partitions=cores, want_terms=False)
+                terms += int(r.n_terms.sum())
+                k += 1
+            if i >= args.warmup:
+                steps_t.append(time.perf_counter() - t0)
+                terms_total += terms
+                inst += k
+        total = sum(steps_t)
+        v = terms_total / total
+        line = dict(base_line, impl="reference", value=v, ms_per_step=1e3 * total / len(steps_t),
+                    cpu_baseline={"value": v, "unit": "terms/s", "cores": cores, "kind": "port",
+                                  "sample": f"{inst} instance runs over {args.steps} steps, oracle with {cores} "
+                                            "partitions/threads, instances one after another"},
+                    e2e={"value": v, "unit": "terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    from propaq_b200 import PauliPropagator, _native
+    from propaq_b200.propagators import expectation_values
+
+    torch.cuda.set_device(local)
+    engine = _native.engine(local)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    keep, items = [], []
+    for p in probs:
+        cfg, k = make_cfg(p, want_terms=False)
+        cfg.blocks_per_sm = args.blocks_per_sm
+        keep.append(k)
+        items.append((cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag))
+    tune = dict(blocks_per_sm=args.blocks_per_sm, split=args.split, rebalance_pct=args.rebalance_pct)
+    jobs = [(PauliPropagator(noise=w.noise(), truncation=w.truncation(), device=local), w.observable, w.circuit,
+             w.initial_state) for w in wls]
+    WM = max(p.n_words for p in probs)
+
+    def settle():
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier(world)
+
+    for _ in range(args.warmup):
+        settle()
+        engine.run_batch(items, **tune)
+    for _ in range(min(1, args.warmup)):
+        settle()
+        expectation_values(jobs, **tune)
+    dev_ms = sweep_ms = 0.0
+    terms = launches = sweep_launches = 0
+    alg_bytes = 0
+    seq_ms, seq_terms, seq_launches = 0.0, 0, 0
+    e2e_s, e2e_terms = 0.0, 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            settle()
+            out = engine.run_batch(items, **tune)
+            torch.cuda.synchronize()
+            dev_ms += out[0][0].device_ms
+            sweep_ms += out[0][0].sweep_ms
+            launches += int(out[0][0].gpu_launches)
+            sweep_launches += max(int(r.sweep_launches) for r, _ in out)
+            for p, (r, nt) in zip(probs, out):
+                terms += int(nt.sum())
+                W = max(p.n_words, WM // 2)
+                alg_bytes += (gate_bytes(W, r.sum_rows_gate, r.sum_anti, r.sum_children) + 8 * W * r.sum_rows_phase
+                              + (8 * W + 16) * (r.sum_rows_noise + r.sum_kept))
+        for _ in range(args.steps):
+            settle()
+            t0 = time.perf_counter()
+            rs = expectation_values(jobs, **tune)
+            torch.cuda.synchronize()
+            e2e_s += time.perf_counter() - t0
+            e2e_terms += sum(sum(r.n_terms) for r in rs)
+        if not args.no_sequential:
+            for _ in range(args.steps):
+                for p, it in zip(probs, items):
+                    settle()
+                    r, nt = engine.run(*it)
+                    seq_ms += r.device_ms
+                    seq_terms += int(nt.sum())
+                    seq_launches += int(r.gpu_launches)
+    clocks = clk.summary()
+    dev_s = max_over_ranks(world, dev_ms / 1e3)
+    e2e_s = max_over_ranks(world, e2e_s)
+    value = world * terms / dev_s
+    h2d = sum(p.obs_keys.nbytes + p.obs_coeffs.nbytes + p.gate_keys.nbytes + p.angles.nbytes + p.offsets.nbytes
+              + (0 if p.diag is None else p.diag.nbytes) + (0 if p.noise_table is None else p.noise_table.nbytes)
+              for p in probs)
+    d2h = sum(8 * len(p.angles) + 16 * (len(p.angles) + len(p.offsets) - 1) + 32 * 4 * 148 for p in probs)
+    peak_gbs, peak_kind = measured_peaks()
+    achieved = alg_bytes / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else None
+    line = dict(base_line, value=value, ms_per_step=1e3 * dev_s / args.steps,
+                instances_per_s=world * len(probs) * args.steps / dev_s,
+                e2e={"value": world * e2e_terms / e2e_s, "unit": "terms/s", "h2d_bytes_per_step": int(h2d),
+                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s / args.steps},
+                gpu_launches=launches // max(1, args.steps),
+                roofline={"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+                          "frac": None if achieved is None else achieved / peak_gbs, "traffic": None,
+                          "kernel": "batch_sweep_kernel", "peak_source": f"{peak_kind} hbm_gbs",
+                          "launches_per_step": sweep_launches / max(1, args.steps),
+                          "share_of_device_time": sweep_ms / dev_ms if dev_ms else None},
+                tuning=tune, clocks=clocks)
+    if seq_ms:
+        line["sequential"] = {"what": "the same 64 instances as pq_run calls one after another, same GPU",
+                              "value": seq_terms / (seq_ms / 1e3), "ms_per_step": seq_ms / args.steps,
+                              "instances_per_s": len(probs) * args.steps / (seq_ms / 1e3),
+                              "gpu_launches_per_step": seq_launches // args.steps}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        o = oracle_load()
+        t0, terms_c, k = time.perf_counter(), 0, 0
+        while k == 0 or time.perf_counter() - t0 < args.cpu_seconds:
+            r = run_oracle(o, probs[k % len(probs)], n_partitions=cores, want_terms=False)
+            terms_c += int(r.n_terms.sum())
+            k += 1
+        el = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": terms_c / el, "unit": "terms/s", "cores": cores, "kind": "port",
+                                "sample": f"the first {k} instance(s) one after another in {el:.1f} s, oracle "
+                                          f"with {cores} partitions/threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def oracle_load():
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_client import Oracle
+
+    return Oracle.load()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
+    if args.workload == "batch":
+        return main_batch(args, world, rank, local)
     wl, desc = make_workload(args.workload)
     cores = os.cpu_count() or 1
     W = 1

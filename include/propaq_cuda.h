@@ -146,6 +146,55 @@ int pq_run(pq_engine* engine, const pq_run_config* cfg, const uint64_t* obs_word
  * Writes min(cap, n) terms, returns n. */
 size_t pq_result_terms(pq_engine* engine, uint64_t* keys, double* coeffs, size_t cap);
 
+/* One propagation of a batch: the arguments of pq_run in one record.  Keys
+ * are pq_words_for_units(cfg.n_units) words wide. */
+typedef struct pq_instance {
+  pq_run_config cfg;
+  const uint64_t* obs_words;
+  const double* obs_coeffs;
+  size_t n_obs;
+  const uint64_t* gate_words;
+  const double* gate_angles;
+  size_t n_gates;
+  const uint32_t* layer_offsets;
+  size_t n_layers;
+  const uint64_t* diag_state;
+  size_t diag_words;
+  uint64_t* n_terms_out;
+  pq_result* result;
+} pq_instance;
+
+/* Grid sharing of pq_run_batch. */
+typedef struct pq_batch_tuning {
+  uint32_t blocks_per_sm;  /* grid size per SM; 0 = as many as fit              */
+  uint32_t split;          /* 0: blocks shared equally among the instances;
+                              1: in proportion to remaining ops x live terms    */
+  uint32_t rebalance_pct;  /* when this % of the grid has been left by finished
+                              instances, the others stop at their next op and
+                              the grid is re-split among them; 0 = never        */
+} pq_batch_tuning;
+
+/* Runs n independent propagations of one basis in shared persistent
+ * launches: each instance owns a slice of the co-resident grid and runs its
+ * op sequence there with its own grid barrier, so small instances fill the
+ * GPU together and no instance pays a launch per gate.  The reference runs
+ * such sweeps as one expectation_value call after another
+ * (ZeroNoiseExtrapolator.run / ZeroCutoffExtrapolator.run,
+ * propaq/extrapolators/zne.py:63-108, zce.py:88-137); each instance's result
+ * is bit-identical to pq_run's on the same arguments.
+ *
+ * Keys up to 2x narrower than the widest instance run at half its width;
+ * narrower ones are widened with zero words (results are unchanged).
+ * device_ms / sweep_ms of every result are the batch's.  A TermBudget floor
+ * together with a weight cut and a weight-changing Clifford rotation needs the
+ * live count on the host mid-run and is refused (PQ_ERR_UNSUPPORTED): run
+ * that instance with pq_run.  tuning NULL = {0, 1, 25}. */
+int pq_run_batch(pq_engine* engine, const pq_instance* instances, size_t n, const pq_batch_tuning* tuning);
+
+/* Final terms of instance `index` of the last batch (index 0 after pq_run),
+ * as pq_result_terms. */
+size_t pq_result_terms_at(pq_engine* engine, size_t index, uint64_t* keys, double* coeffs, size_t cap);
+
 /* Plugins: the reference's loader and validation, byte for byte the same
  * symbol names (crates/core/src/policy/native_noise.rs:217-288,
  * crates/core/src/policy/native_truncator.rs:205-276). */

@@ -85,6 +85,32 @@ _V = ctypes.c_void_p
 _Z = ctypes.c_size_t
 _U32 = ctypes.c_uint32
 
+class Instance(ctypes.Structure):
+    """pq_instance: one propagation of a pq_run_batch call."""
+
+    _fields_ = [
+        ("cfg", RunConfig),
+        ("obs_words", _V),
+        ("obs_coeffs", _V),
+        ("n_obs", _Z),
+        ("gate_words", _V),
+        ("gate_angles", _V),
+        ("n_gates", _Z),
+        ("layer_offsets", _V),
+        ("n_layers", _Z),
+        ("diag_state", _V),
+        ("diag_words", _Z),
+        ("n_terms_out", _V),
+        ("result", ctypes.POINTER(RunResult)),
+    ]
+
+
+class BatchTuning(ctypes.Structure):
+    """pq_batch_tuning."""
+
+    _fields_ = [("blocks_per_sm", ctypes.c_uint32), ("split", ctypes.c_uint32), ("rebalance_pct", ctypes.c_uint32)]
+
+
 _SIGNATURES = {
     "pq_words_for_units": (_U32, [_U32]),
     "pq_engine_create": (ctypes.c_int, [ctypes.POINTER(_V), ctypes.c_int]),
@@ -93,6 +119,8 @@ _SIGNATURES = {
     "pq_run": (ctypes.c_int, [_V, ctypes.POINTER(RunConfig), _V, _V, _Z, _V, _V, _Z, _V, _Z, _V, _Z, _V,
                               ctypes.POINTER(RunResult)]),
     "pq_result_terms": (_Z, [_V, _V, _V, _Z]),
+    "pq_run_batch": (ctypes.c_int, [_V, ctypes.POINTER(Instance), _Z, ctypes.POINTER(BatchTuning)]),
+    "pq_result_terms_at": (_Z, [_V, _Z, _V, _V, _Z]),
     "pq_plugin_load_noise": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_V),
                                             ctypes.c_char_p, _Z]),
     "pq_plugin_load_truncator": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_V),
@@ -177,14 +205,48 @@ class Engine:
                 raise_for(rc, lib().pq_engine_last_error(self._h).decode(errors="replace"))
         return res, nt
 
-    def terms(self, n_words: int):
-        """Final (keys, coeffs) of the last run made with want_terms."""
+    def run_batch(self, items, blocks_per_sm: int = 0, split: int = 1, rebalance_pct: int = 25,
+                  want_n_terms: bool = True):
+        """Runs pq_run_batch on a list of (cfg, obs_words, obs_coeffs, gate_words,
+        gate_angles, layer_offsets, diag_state) tuples; returns one
+        (RunResult, n_terms array or None) per instance."""
+        keep = []
+        insts = (Instance * len(items))()
+        out = []
+        for inst, (cfg, ow, oc, gw, ga, lo, diag) in zip(insts, items):
+            ow = np.ascontiguousarray(ow, dtype=np.uint64)
+            oc = np.ascontiguousarray(oc, dtype=np.float64)
+            gw = np.ascontiguousarray(gw, dtype=np.uint64)
+            ga = np.ascontiguousarray(ga, dtype=np.float64)
+            lo = np.ascontiguousarray(lo, dtype=np.uint32)
+            diag = None if diag is None else np.ascontiguousarray(diag, dtype=np.uint64)
+            nt = np.zeros(len(ga), dtype=np.uint64) if want_n_terms else None
+            res = RunResult()
+            keep += [ow, oc, gw, ga, lo, diag, nt, res]
+            inst.cfg = cfg
+            inst.obs_words, inst.obs_coeffs, inst.n_obs = _ptr(ow), _ptr(oc), len(oc)
+            inst.gate_words, inst.gate_angles, inst.n_gates = _ptr(gw), _ptr(ga), len(ga)
+            inst.layer_offsets, inst.n_layers = _ptr(lo), len(lo) - 1
+            inst.diag_state, inst.diag_words = _ptr(diag), 0 if diag is None else len(diag)
+            inst.n_terms_out = _ptr(nt)
+            inst.result = ctypes.pointer(res)
+            out.append((res, nt))
         with self.lock:
-            n = lib().pq_result_terms(self._h, None, None, 0)
+            tune = BatchTuning(blocks_per_sm, split, rebalance_pct)
+            rc = lib().pq_run_batch(self._h, insts, len(items), ctypes.byref(tune))
+            if rc != PQ_OK:
+                raise_for(rc, lib().pq_engine_last_error(self._h).decode(errors="replace"))
+        return out
+
+    def terms(self, n_words: int, index: int = 0):
+        """Final (keys, coeffs) of the last run made with want_terms (instance
+        `index` of the last batch)."""
+        with self.lock:
+            n = lib().pq_result_terms_at(self._h, index, None, None, 0)
             keys = np.zeros((n, n_words), dtype=np.uint64)
             coeffs = np.zeros(n, dtype=np.float64)
             if n:
-                lib().pq_result_terms(self._h, _ptr(keys), _ptr(coeffs), n)
+                lib().pq_result_terms_at(self._h, index, _ptr(keys), _ptr(coeffs), n)
         return keys, coeffs
 
 

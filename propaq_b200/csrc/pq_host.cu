@@ -13,11 +13,11 @@
 // sin/cos/exp are evaluated here with the host libm, the same glibc the
 // reference calls, so the device sees bit-identical factors.
 //
-// Ops are enqueued without waiting for the device.  Each gate kernel first
-// checks that twice the live count fits the row capacity; if not, it and every
-// later op skip themselves and record where they stopped.  The host notices at
-// its next synchronisation, grows the buffers, rebuilds the hash table and
-// replays the ops from the one that stopped.
+// The device side is one cooperative persistent launch per propagation (or
+// per batch of propagations) that runs the whole op sequence with grid
+// barriers between ops.  A gate that would need more rows than the buffers
+// hold stops the launch and records where; the host grows the buffers,
+// rebuilds the hash table and relaunches from that op.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 
@@ -27,6 +27,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -321,13 +322,22 @@ u64 next_pow2(u64 x) {
 }  // namespace
 
 // ---------------------------------------------------------------- engine
-struct pq_engine {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_l0 = nullptr, ev_l1 = nullptr;
-  std::string err;
-  pq::SweepState* st = nullptr;    // device
-  pq::SweepState* h_st = nullptr;  // pinned mirror
+namespace {
+
+// Calls f(std::integral_constant<int, W>) for a compiled key width.
+template <class F>
+decltype(auto) with_words(int W, F&& f) {
+  switch (W) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    default: return f(std::integral_constant<int, 8>{});
+  }
+}
+
+// Device resources of one propagation.  Slot 0 serves pq_run; a batch uses
+// slots 0..n-1.  Buffers grow on demand and are kept for the next run.
+struct Slot {
   u64* keys[2] = {nullptr, nullptr};
   double* coeffs[2] = {nullptr, nullptr};
   u64* table = nullptr;
@@ -337,7 +347,6 @@ struct pq_engine {
   int W = 0;
   int cur = 0;
   u32 epoch_base = 1;
-  // per-op device arrays
   size_t ops_cap = 0;
   pq::OpDesc* d_ops = nullptr;
   u32* tickets = nullptr;
@@ -349,21 +358,13 @@ struct pq_engine {
   double* d_tables = nullptr;
   size_t d_tables_cap = 0;
   pq::ExpectPartial* partials = nullptr;
-  int expect_grid = 0;
-  u32* d_err = nullptr;  // error word of the stand-alone kernels
+  u64* frame_img = nullptr;  // readout tableau of the last run, when not the identity
+  int* frame_sgn = nullptr;
+  size_t frame_cap = 0;
+  int out_words = 0;  // width of out_keys (the caller's width)
   std::vector<u64> out_keys;
   std::vector<double> out_coeffs;
-  u64 launches = 0;
 
-  int fail(int code, const std::string& m) {
-    err = m;
-    return code;
-  }
-  int cuda_fail(cudaError_t e, const char* what) {
-    cudaGetLastError();
-    return fail(e == cudaErrorMemoryAllocation ? PQ_ERR_OOM : PQ_ERR_CUDA,
-                std::string(what) + ": " + cudaGetErrorString(e));
-  }
   void free_rows() {
     for (int i = 0; i < 2; ++i) {
       if (keys[i]) cudaFree(keys[i]);
@@ -385,20 +386,93 @@ struct pq_engine {
     hist = anti = stamps = nullptr;
     ops_cap = 0;
   }
-  ~pq_engine() {
-    if (stream) cudaStreamSynchronize(stream);
+  void free_all() {
     free_rows();
     free_ops();
-    for (void* p : {(void*)st, (void*)d_gates, (void*)d_tables, (void*)partials, (void*)d_err})
+    for (void* p : {(void*)d_gates, (void*)d_tables, (void*)partials, (void*)frame_img, (void*)frame_sgn})
       if (p) cudaFree(p);
-    if (h_st) cudaFreeHost(h_st);
+    d_gates = nullptr;
+    d_tables = nullptr;
+    partials = nullptr;
+    frame_img = nullptr;
+    frame_sgn = nullptr;
+    gates_bytes = d_tables_cap = frame_cap = 0;
+  }
+};
+
+// Grows a device array (and its pinned host mirror, when `host` is given) to
+// hold n elements.
+template <class T>
+cudaError_t grow_pair(T** dev, T** host, size_t* cap, size_t n) {
+  if (*cap >= n) return cudaSuccess;
+  if (*dev) cudaFree(*dev);
+  if (host && *host) cudaFreeHost(*host);
+  *dev = nullptr;
+  if (host) *host = nullptr;
+  *cap = 0;
+  cudaError_t e = cudaMalloc(dev, n * sizeof(T));
+  if (e == cudaSuccess && host) e = cudaMallocHost(host, n * sizeof(T));
+  if (e == cudaSuccess) *cap = n;
+  return e;
+}
+
+}  // namespace
+
+struct pq_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_l0 = nullptr, ev_l1 = nullptr;
+  std::string err;
+  std::vector<Slot> slots;
+  pq::SweepState* d_states = nullptr;  // one per slot
+  pq::SweepState* h_states = nullptr;  // pinned mirror
+  size_t states_cap = 0;
+  pq::SweepArgs* d_args = nullptr;  // per instance of a batched launch
+  pq::SweepArgs* h_args = nullptr;
+  size_t args_cap = 0;
+  u32* d_block_inst = nullptr;  // instance of each block of a batched launch
+  u32* h_block_inst = nullptr;
+  size_t block_inst_cap = 0;
+  int expect_grid = 0;
+  u32* d_err = nullptr;   // error word of the stand-alone kernels
+  u32* d_idle = nullptr;  // blocks left idle in a batched launch
+  u64 launches = 0;
+
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char* what) {
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? PQ_ERR_OOM : PQ_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+  }
+  ~pq_engine() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& s : slots) s.free_all();
+    for (void* p : {(void*)d_states, (void*)d_args, (void*)d_block_inst, (void*)d_err, (void*)d_idle})
+      if (p) cudaFree(p);
+    for (void* p : {(void*)h_states, (void*)h_args, (void*)h_block_inst})
+      if (p) cudaFreeHost(p);
     for (auto ev : {ev_begin, ev_end, ev_l0, ev_l1})
       if (ev) cudaEventDestroy(ev);
     if (stream) cudaStreamDestroy(stream);
   }
-  // (Re)allocates rows for `new_cap`, keeping the first n live rows of buffer
-  // `from` in buffer 0, then clears and rebuilds the table.  Synchronous.
-  int resize(u64 new_cap, u64 n, int from, int Wn) {
+  int ensure_slots(size_t n) {
+    if (slots.size() < n) slots.resize(n);
+    if (cudaError_t e = grow_pair(&d_states, &h_states, &states_cap, n)) return cuda_fail(e, "sweep states");
+    return PQ_OK;
+  }
+  int ensure_batch_arrays(size_t n_args, size_t n_blocks) {
+    if (cudaError_t e = grow_pair(&d_args, &h_args, &args_cap, n_args)) return cuda_fail(e, "batch arguments");
+    if (cudaError_t e = grow_pair(&d_block_inst, &h_block_inst, &block_inst_cap, n_blocks))
+      return cuda_fail(e, "batch block map");
+    return PQ_OK;
+  }
+  // (Re)allocates a slot's rows for `new_cap`, keeping the first n live rows
+  // of buffer `from` in buffer 0, then clears and rebuilds the table.
+  // Synchronous.
+  int resize(Slot& S, u64 new_cap, u64 n, int from, int Wn) {
     cudaError_t e;
     u64* nk[2] = {nullptr, nullptr};
     double* nc[2] = {nullptr, nullptr};
@@ -425,50 +499,47 @@ struct pq_engine {
       cleanup();
       return cuda_fail(e, "allocating the hash table");
     }
-    if (n && keys[from]) {
-      cudaMemcpyAsync(nk[0], keys[from], n * Wn * 8, cudaMemcpyDeviceToDevice, stream);
-      cudaMemcpyAsync(nc[0], coeffs[from], n * 8, cudaMemcpyDeviceToDevice, stream);
+    if (n && S.keys[from]) {
+      cudaMemcpyAsync(nk[0], S.keys[from], n * Wn * 8, cudaMemcpyDeviceToDevice, stream);
+      cudaMemcpyAsync(nc[0], S.coeffs[from], n * 8, cudaMemcpyDeviceToDevice, stream);
     }
     cudaMemsetAsync(ns, 0, n_status * 8, stream);
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) {
       cleanup();
       return cuda_fail(e, "copying rows");
     }
-    free_rows();
-    keys[0] = nk[0];
-    keys[1] = nk[1];
-    coeffs[0] = nc[0];
-    coeffs[1] = nc[1];
-    table = nt;
-    status = ns;
-    cap = new_cap;
-    tcap = ntcap;
-    cur = 0;
-    W = Wn;
-    return rebuild_table(n);
+    S.free_rows();
+    S.keys[0] = nk[0];
+    S.keys[1] = nk[1];
+    S.coeffs[0] = nc[0];
+    S.coeffs[1] = nc[1];
+    S.table = nt;
+    S.status = ns;
+    S.cap = new_cap;
+    S.tcap = ntcap;
+    S.cur = 0;
+    S.W = Wn;
+    return rebuild_table(S, n);
   }
-  int rebuild_table(u64 n) {
-    cudaMemsetAsync(table, 0xff, tcap * 8, stream);
-    cudaError_t e;
-    switch (W) {
-      case 1: e = pq::launch_rebuild<1>(keys[cur], n, table, tcap - 1, d_err, stream); break;
-      case 2: e = pq::launch_rebuild<2>(keys[cur], n, table, tcap - 1, d_err, stream); break;
-      case 4: e = pq::launch_rebuild<4>(keys[cur], n, table, tcap - 1, d_err, stream); break;
-      default: e = pq::launch_rebuild<8>(keys[cur], n, table, tcap - 1, d_err, stream); break;
-    }
+  int rebuild_table(Slot& S, u64 n) {
+    cudaMemsetAsync(S.table, 0xff, S.tcap * 8, stream);
+    const cudaError_t e = with_words(S.W, [&](auto w) {
+      return pq::launch_rebuild<decltype(w)::value>(S.keys[S.cur], n, S.table, S.tcap - 1, d_err, stream);
+    });
     if (n) ++launches;
     if (e != cudaSuccess) return cuda_fail(e, "rebuild launch");
     return PQ_OK;
   }
-  int ensure_ops(size_t n_ops) {
-    if (ops_cap >= n_ops) return PQ_OK;
-    free_ops();
+  int ensure_ops(Slot& S, size_t n_ops) {
+    if (S.ops_cap >= n_ops) return PQ_OK;
+    S.free_ops();
     cudaError_t e;
-    if ((e = cudaMalloc(&d_ops, n_ops * sizeof(pq::OpDesc))) != cudaSuccess ||
-        (e = cudaMalloc(&tickets, n_ops * 4)) != cudaSuccess || (e = cudaMalloc(&hist, n_ops * 8)) != cudaSuccess ||
-        (e = cudaMalloc(&anti, n_ops * 8)) != cudaSuccess || (e = cudaMalloc(&stamps, n_ops * 8)) != cudaSuccess)
+    if ((e = cudaMalloc(&S.d_ops, n_ops * sizeof(pq::OpDesc))) != cudaSuccess ||
+        (e = cudaMalloc(&S.tickets, n_ops * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&S.hist, n_ops * 8)) != cudaSuccess || (e = cudaMalloc(&S.anti, n_ops * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&S.stamps, n_ops * 8)) != cudaSuccess)
       return cuda_fail(e, "allocating op arrays");
-    ops_cap = n_ops;
+    S.ops_cap = n_ops;
     return PQ_OK;
   }
 };
@@ -498,45 +569,102 @@ pq::GenInfo<W> make_gen(int alg, const u64* g, int sign) {
   return gi;
 }
 
-template <int W, int ALG>
-int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const double* obs_coeffs, size_t n_obs,
-             const u64* gate_words, const double* angles, size_t n_gates, const u32* layer_off, size_t n_layers,
-             const u64* diag, size_t nd, u64* n_terms_out, pq_result* res) {
-  const u32 n_units = cfg->n_units;
-  const bool has_w = cfg->max_weight >= 0;
-  const u32 wcut = has_w ? (u32)std::min<int64_t>(cfg->max_weight, 0xfffffffe) : pq::NO_WEIGHT_CUT;
-  const bool has_c = cfg->has_min_coeff != 0;
-  const double ccut = cfg->min_coeff;
-  const bool has_floor = cfg->min_terms >= 0;
-  const u64 floor_terms = has_floor ? (u64)cfg->min_terms : 0;
-  cudaError_t e;
+// One propagation's inputs as the C ABI receives them; keys are `in_words`
+// words wide (pq_words_for_units of the instance).
+struct Inputs {
+  const pq_run_config* cfg;
+  const u64* obs_words;
+  const double* obs_coeffs;
+  size_t n_obs;
+  const u64* gate_words;
+  const double* angles;
+  size_t n_gates;
+  const u32* layer_off;
+  size_t n_layers;
+  const u64* diag;
+  size_t nd;
+  u64* n_terms_out;
+  pq_result* res;
+  int in_words;
+};
 
-  // Noise resolution (noise_resolver.rs:78-131): one factor table per layer
-  // or one for the run.
-  const Plugin* np = reinterpret_cast<const Plugin*>(cfg->noise_plugin);
-  size_t tlen = cfg->noise_table_len ? cfg->noise_table_len : (size_t)n_units + 1;
+// Host side of one propagation: resolved noise, the admitted observable, the
+// op sequence with its gate descriptors, the Clifford frame, and how far the
+// device has run it.  W is the width the device runs it at (>= in_words; the
+// extra words are zero).
+struct Plan {
+  const Inputs* in = nullptr;
+  int W = 1, alg = 0;
+  u32 n_units = 0;
+  bool has_w = false, has_c = false, has_floor = false;
+  u32 wcut = pq::NO_WEIGHT_CUT;
+  double ccut = 0;
+  u64 floor_terms = 0;
+  size_t tlen = 0;
   std::vector<double> tables;
-  bool layered = false;
-  const bool have_noise = cfg->noise_kind != PQ_NOISE_NONE;
+  bool layered = false, have_noise = false;
+  std::vector<u64> hk;
+  std::vector<double> hc;
+  u64 n0 = 0;
+  std::vector<pq::OpDesc> ops;
+  std::vector<u64> gdesc;  // GateDesc<W> records back to back
+  size_t n_gdesc = 0;
+  std::vector<long> gate_op;  // latest op at or before each gate, -1 = none
+  Tableau frame{0, 1, 0};
+  long last_op = -1;
+  size_t done = 0, uploaded_ops = 0, uploaded_gdesc = 0;
+  u64 n_live = 0, peak = 0;
+  double sweep_ms = 0;
+  u64 sweep_launches = 0;
+
+  // Copies key i of an input array (in_words wide) into W words.
+  void widen(const u64* src, size_t i, u64* dst) const {
+    for (int w = 0; w < W; ++w) dst[w] = w < in->in_words ? src[i * in->in_words + w] : 0;
+  }
+};
+
+size_t gdesc_words(int W) {
+  return with_words(W, [](auto w) { return sizeof(pq::GateDesc<decltype(w)::value>) / 8; });
+}
+
+// Resolves noise (noise_resolver.rs:78-131) and admits the observable with
+// duplicate folding (engine.rs:104-111).
+int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
+  const pq_run_config* cfg = in.cfg;
+  P.in = &in;
+  P.W = W;
+  P.alg = (int)cfg->basis_kind;
+  const int ALG = P.alg;
+  P.n_units = cfg->n_units;
+  P.has_w = cfg->max_weight >= 0;
+  P.wcut = P.has_w ? (u32)std::min<int64_t>(cfg->max_weight, 0xfffffffe) : pq::NO_WEIGHT_CUT;
+  P.has_c = cfg->has_min_coeff != 0;
+  P.ccut = cfg->min_coeff;
+  P.has_floor = cfg->min_terms >= 0;
+  P.floor_terms = P.has_floor ? (u64)cfg->min_terms : 0;
+  const Plugin* np = reinterpret_cast<const Plugin*>(cfg->noise_plugin);
+  P.tlen = cfg->noise_table_len ? cfg->noise_table_len : (size_t)P.n_units + 1;
+  P.have_noise = cfg->noise_kind != PQ_NOISE_NONE;
   if (cfg->noise_kind == PQ_NOISE_TABLE) {
     if (!cfg->noise_tables || !cfg->noise_table_len) return E->fail(PQ_ERR_INVALID, "noise table missing");
-    tables.assign(cfg->noise_tables, cfg->noise_tables + tlen);
+    P.tables.assign(cfg->noise_tables, cfg->noise_tables + P.tlen);
   } else if (cfg->noise_kind == PQ_NOISE_LAYERED) {
     if (!cfg->noise_tables || !cfg->noise_table_len) return E->fail(PQ_ERR_INVALID, "noise tables missing");
-    tables.assign(cfg->noise_tables, cfg->noise_tables + tlen * n_layers);
-    layered = true;
+    P.tables.assign(cfg->noise_tables, cfg->noise_tables + P.tlen * in.n_layers);
+    P.layered = true;
   } else if (cfg->noise_kind == PQ_NOISE_PLUGIN) {
     if (!np) return E->fail(PQ_ERR_INVALID, "noise plugin missing");
     if (np->depends & 1)
       return E->fail(PQ_ERR_UNSUPPORTED, "key-reading noise plugins are not run by the CUDA engine yet");
-    tlen = (size_t)n_units + 1;
+    P.tlen = (size_t)P.n_units + 1;
     auto f = (NoiseFactorFn)np->fn;
     auto tab = [&](u32 layer, u32 total) {
-      for (u32 w = 0; w < n_units + 1; ++w) tables.push_back(f(np->ctx, ALG, nullptr, 0, n_units, w, layer, total));
+      for (u32 w = 0; w < P.n_units + 1; ++w)
+        P.tables.push_back(f(np->ctx, ALG, nullptr, 0, P.n_units, w, layer, total));
     };
     if (np->depends & 2) {
-      layered = true;
-      for (size_t l = 0; l < n_layers; ++l) tab((u32)l, (u32)n_layers);
+      P.layered = true;
+      for (size_t l = 0; l < in.n_layers; ++l) tab((u32)l, (u32)in.n_layers);
     } else {
       tab(0, 0);
     }
@@ -545,264 +673,338 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
   }
   if (cfg->truncator)
     return E->fail(PQ_ERR_UNSUPPORTED, "native truncator plugins are not run by the CUDA engine yet");
-
-  // Observable admission with duplicate folding (engine.rs:104-111).
-  std::vector<u64> hk;
-  std::vector<double> hc;
-  {
-    struct H {
-      size_t operator()(const std::vector<u64>& v) const { return (size_t)pq::key_hash<W>(v.data()); }
-    };
-    std::unordered_map<std::vector<u64>, size_t, H> pos;
-    std::vector<u64> k(W);
-    for (size_t i = 0; i < n_obs; ++i) {
-      std::memcpy(k.data(), obs_words + i * W, 8 * W);
-      const double c = obs_coeffs[i];
-      if (has_w && host_weight(ALG, W, k.data(), n_units) > wcut) continue;
-      if (has_c && !(std::fabs(c) >= ccut)) continue;
-      auto it = pos.find(k);
-      if (it != pos.end()) {
-        hc[it->second] += c;
-      } else {
-        pos.emplace(k, hc.size());
-        hk.insert(hk.end(), k.begin(), k.end());
-        hc.push_back(c);
+  struct H {
+    size_t operator()(const std::vector<u64>& v) const {
+      u64 h = 0x9e3779b97f4a7c15ULL;
+      for (u64 x : v) {
+        h = (h ^ x) * 0xff51afd7ed558ccdULL;
+        h ^= h >> 29;
       }
+      return (size_t)h;
     }
-  }
-  const u64 n0 = hc.size();
-
-  // Device set-up: rows, table, op arrays, noise tables.
-  const u64 want_cap = next_pow2(std::max<u64>(4 * n0, 1ULL << 16));
-  if (E->W != W || E->cap < want_cap) {
-    if (int rc = E->resize(std::max(want_cap, E->cap), 0, E->cur, W)) return rc;
-  }
-  E->cur = 0;
-  if (n0) {
-    cudaMemcpyAsync(E->keys[0], hk.data(), n0 * W * 8, cudaMemcpyHostToDevice, E->stream);
-    cudaMemcpyAsync(E->coeffs[0], hc.data(), n0 * 8, cudaMemcpyHostToDevice, E->stream);
-  }
-  if (int rc = E->rebuild_table(n0)) return rc;
-  const size_t n_ops_max = n_gates + n_layers + 1;
-  if (int rc = E->ensure_ops(n_ops_max)) return rc;
-  const size_t gbytes = std::max<size_t>(n_gates, 1) * sizeof(pq::GateDesc<W>);
-  if (E->gates_bytes < gbytes) {
-    if (E->d_gates) cudaFree(E->d_gates);
-    E->d_gates = nullptr;
-    if ((e = cudaMalloc(&E->d_gates, gbytes)) != cudaSuccess) return E->cuda_fail(e, "gate descriptors");
-    E->gates_bytes = gbytes;
-  }
-  if (!tables.empty() && E->d_tables_cap < tables.size()) {
-    if (E->d_tables) cudaFree(E->d_tables);
-    E->d_tables = nullptr;
-    if ((e = cudaMalloc(&E->d_tables, tables.size() * 8)) != cudaSuccess) return E->cuda_fail(e, "noise tables");
-    E->d_tables_cap = tables.size();
-  }
-  if (!tables.empty())
-    cudaMemcpyAsync(E->d_tables, tables.data(), tables.size() * 8, cudaMemcpyHostToDevice, E->stream);
-  cudaMemsetAsync(E->anti, 0, n_ops_max * 8, E->stream);
-  if (E->epoch_base > (1u << 29)) {  // keep status tags unique: restart the epochs on a cleared array
-    E->epoch_base = 1;
-    cudaMemsetAsync(E->status, 0, (E->cap / TILE_ROWS + 2) * 8, E->stream);
-  }
-
-  std::vector<pq::OpDesc> ops;
-  std::vector<pq::GateDesc<W>> gdesc;
-  ops.reserve(n_ops_max);
-  gdesc.reserve(n_gates);
-  std::vector<long> gate_op(n_gates, -1);  // latest op at or before each gate
-  u64 n_live = n0, peak = n0;
-  size_t done = 0;  // ops executed so far
-  size_t gdone = 0; // gate descriptors uploaded so far
-  const int grid = pq::sweep_grid<W, ALG>((int)cfg->blocks_per_sm);
-  double sweep_ms = 0;
-  u64 sweep_launches = 0;
-  bool began = false;
-
-  // Runs ops [done, ops.size()) on the device; on a capacity halt grows the
-  // rows and relaunches from the halted op.
-  auto flush = [&]() -> int {
-    if (ops.size() > done) {
-      cudaMemcpyAsync(E->d_ops + done, ops.data() + done, (ops.size() - done) * sizeof(pq::OpDesc),
-                      cudaMemcpyHostToDevice, E->stream);
-    }
-    if (gdesc.size() > gdone) {
-      cudaMemcpyAsync(reinterpret_cast<pq::GateDesc<W>*>(E->d_gates) + gdone, gdesc.data() + gdone,
-                      (gdesc.size() - gdone) * sizeof(pq::GateDesc<W>), cudaMemcpyHostToDevice, E->stream);
-      gdone = gdesc.size();
-    }
-    while (done < ops.size()) {
-      pq::SweepState s{};
-      s.n[done & 1] = n_live;
-      s.peak = peak;
-      s.halt = pq::NOT_HALTED;
-      s.bar_gen = 0;
-      *E->h_st = s;
-      cudaMemcpyAsync(E->st, E->h_st, sizeof s, cudaMemcpyHostToDevice, E->stream);
-      cudaMemsetAsync(E->tickets + done, 0, (ops.size() - done) * 4, E->stream);
-      pq::SweepArgs a{};
-      a.ops = E->d_ops;
-      a.gates = E->d_gates;
-      a.tables = E->d_tables;
-      a.table_len = (u32)tlen;
-      a.n_units = n_units;
-      a.op_begin = (u32)done;
-      a.op_end = (u32)ops.size();
-      a.cur0 = (u32)E->cur;
-      a.epoch_base = E->epoch_base;
-      a.max_weight = wcut;
-      a.has_min_coeff = has_c;
-      a.min_coeff = ccut;
-      a.min_terms = floor_terms;
-      for (int i = 0; i < 2; ++i) {
-        a.keys[i] = E->keys[i];
-        a.coeffs[i] = E->coeffs[i];
-      }
-      a.table = E->table;
-      a.table_mask = E->tcap - 1;
-      a.cap = E->cap;
-      a.status = E->status;
-      a.tickets = E->tickets;
-      a.hist = E->hist;
-      a.anti = E->anti;
-      a.stamps = E->stamps;
-      a.st = E->st;
-      if (!began) {  // device time starts at the first sweep
-        cudaEventRecord(E->ev_begin, E->stream);
-        began = true;
-      }
-      cudaEventRecord(E->ev_l0, E->stream);
-      if ((e = pq::launch_sweep<W, ALG>(a, grid, E->stream)) != cudaSuccess) return E->cuda_fail(e, "sweep launch");
-      cudaEventRecord(E->ev_l1, E->stream);
-      ++E->launches;
-      ++sweep_launches;
-      E->epoch_base += (u32)ops.size() + 1;
-      cudaMemcpyAsync(E->h_st, E->st, sizeof s, cudaMemcpyDeviceToHost, E->stream);
-      if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "sweep");
-      float ms = 0;
-      cudaEventElapsedTime(&ms, E->ev_l0, E->ev_l1);
-      sweep_ms += ms;
-      const pq::SweepState h = *E->h_st;
-      if (h.error & pq::ERR_BARRIER_TIMEOUT)
-        return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a grid barrier wait expired on the device");
-      if (h.error & pq::ERR_LOOKBACK_TIMEOUT)
-        return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a tile's look-back wait expired on the device");
-      if (h.error) return E->fail(PQ_ERR_CUDA, "device reported error bits " + std::to_string(h.error));
-      E->cur = (int)h.cur;
-      done = h.end_op;
-      n_live = h.n[done & 1];
-      peak = std::max(peak, h.peak);
-      if (h.halt != pq::NOT_HALTED) {  // grow: the gate at `done` needs 2 N rows
-        u64 ncap = next_pow2(std::max<u64>(4 * n_live, 2 * E->cap));
-        if (ncap > MAX_ROWS) ncap = MAX_ROWS;
-        if (2 * n_live > ncap)
-          return E->fail(PQ_ERR_CEILING, "term index ceiling reached: " + std::to_string(2 * n_live) +
-                                             " rows would exceed the engine's capacity");
-        int rc = E->resize(ncap, n_live, E->cur, W);
-        if (rc == PQ_ERR_OOM) rc = E->resize(next_pow2(2 * n_live), n_live, E->cur, W);
-        if (rc) return rc;
-      }
-    }
-    return PQ_OK;
   };
-
-  Tableau frame(ALG, W, n_units);
-  std::vector<u64> g(W), gc(W);
-  long last_op = -1;
-  for (size_t l = 0; l < n_layers; ++l) {
-    if (have_noise) {
-      pq::OpDesc od;
-      od.kind = (has_w || has_c) ? pq::OP_NOISE_COMPACT : pq::OP_NOISE_SCALE;  // partitioned_termsum.rs:585-587
-      od.idx = layered ? (u32)l : 0u;
-      ops.push_back(od);
-      last_op = (long)ops.size() - 1;
+  std::unordered_map<std::vector<u64>, size_t, H> pos;
+  std::vector<u64> k(W);
+  for (size_t i = 0; i < in.n_obs; ++i) {
+    P.widen(in.obs_words, i, k.data());
+    const double c = in.obs_coeffs[i];
+    if (P.has_w && host_weight(ALG, W, k.data(), P.n_units) > P.wcut) continue;
+    if (P.has_c && !(std::fabs(c) >= P.ccut)) continue;
+    auto it = pos.find(k);
+    if (it != pos.end()) {
+      P.hc[it->second] += c;
+    } else {
+      pos.emplace(k, P.hc.size());
+      P.hk.insert(P.hk.end(), k.begin(), k.end());
+      P.hc.push_back(c);
     }
-    for (u32 gi = layer_off[l]; gi < layer_off[l + 1]; ++gi) {
-      std::memcpy(g.data(), gate_words + (size_t)gi * W, 8 * W);
-      const double ang = angles[gi];
+  }
+  P.n0 = P.hc.size();
+  P.n_live = P.peak = P.n0;
+  P.frame = Tableau(ALG, W, P.n_units);
+  P.gate_op.assign(in.n_gates, -1);
+  P.ops.reserve(in.n_gates + in.n_layers);
+  P.gdesc.reserve(in.n_gates * gdesc_words(W));
+  return PQ_OK;
+}
+
+// Sizes the slot's buffers for the plan, uploads the admitted rows and noise
+// tables, rebuilds the table.
+int setup_slot(pq_engine* E, Slot& S, Plan& P) {
+  cudaError_t e;
+  const int W = P.W;
+  const u64 want_cap = next_pow2(std::max<u64>(4 * P.n0, 1ULL << 16));
+  if (S.W != W || S.cap < want_cap) {
+    if (int rc = E->resize(S, std::max(want_cap, S.W == W ? S.cap : 0), 0, S.cur, W)) return rc;
+  }
+  S.cur = 0;
+  if (P.n0) {
+    cudaMemcpyAsync(S.keys[0], P.hk.data(), P.n0 * W * 8, cudaMemcpyHostToDevice, E->stream);
+    cudaMemcpyAsync(S.coeffs[0], P.hc.data(), P.n0 * 8, cudaMemcpyHostToDevice, E->stream);
+  }
+  if (int rc = E->rebuild_table(S, P.n0)) return rc;
+  const size_t n_ops_max = P.in->n_gates + P.in->n_layers + 1;
+  if (int rc = E->ensure_ops(S, n_ops_max)) return rc;
+  const size_t gbytes = std::max<size_t>(P.in->n_gates, 1) * gdesc_words(W) * 8;
+  if (S.gates_bytes < gbytes) {
+    if (S.d_gates) cudaFree(S.d_gates);
+    S.d_gates = nullptr;
+    S.gates_bytes = 0;
+    if ((e = cudaMalloc(&S.d_gates, gbytes)) != cudaSuccess) return E->cuda_fail(e, "gate descriptors");
+    S.gates_bytes = gbytes;
+  }
+  if (!P.tables.empty()) {
+    if ((e = grow_pair<double>(&S.d_tables, nullptr, &S.d_tables_cap, P.tables.size())) != cudaSuccess)
+      return E->cuda_fail(e, "noise tables");
+    cudaMemcpyAsync(S.d_tables, P.tables.data(), P.tables.size() * 8, cudaMemcpyHostToDevice, E->stream);
+  }
+  if (!S.partials) {
+    if ((e = cudaMalloc(&S.partials, sizeof(pq::ExpectPartial) * E->expect_grid)) != cudaSuccess)
+      return E->cuda_fail(e, "partials");
+  }
+  cudaMemsetAsync(S.anti, 0, n_ops_max * 8, E->stream);
+  if (S.epoch_base > (1u << 29)) {  // keep status tags unique: restart the epochs on a cleared array
+    S.epoch_base = 1;
+    cudaMemsetAsync(S.status, 0, (S.cap / TILE_ROWS + 2) * 8, E->stream);
+  }
+  return PQ_OK;
+}
+
+// Appends the op sequence (engine.rs:117-205, partitioned_termsum.rs:282-350).
+// need_n(&n) is called when the Clifford deferral decision depends on the
+// live count (TermBudget with a weight cut); it must run the ops built so far
+// and report the live count.
+template <class NeedN>
+int build_ops(Plan& P, NeedN need_n) {
+  const Inputs& in = *P.in;
+  const int W = P.W, ALG = P.alg;
+  std::vector<u64> g(W), gc(W);
+  for (size_t l = 0; l < in.n_layers; ++l) {
+    if (P.have_noise) {
+      pq::OpDesc od;
+      od.kind = (P.has_w || P.has_c) ? pq::OP_NOISE_COMPACT : pq::OP_NOISE_SCALE;  // partitioned_termsum.rs:585-587
+      od.idx = P.layered ? (u32)l : 0u;
+      P.ops.push_back(od);
+      P.last_op = (long)P.ops.size() - 1;
+    }
+    for (u32 gi = in.layer_off[l]; gi < in.layer_off[l + 1]; ++gi) {
+      P.widen(in.gate_words, gi, g.data());
+      const double ang = in.angles[gi];
       if (std::fabs(std::cos(ang)) < EPS_CLASSIFY) {  // Clifford: defer into the frame when allowed
-        bool eff_w = has_w;
-        const bool cw = Tableau::rotation_changes_weight(ALG, W, n_units, g.data());
-        if (has_w && cw && has_floor) {  // the effective cutoff depends on the live count here
-          if (int rc = flush()) return rc;
-          if (n_live < floor_terms) eff_w = false;
+        bool eff_w = P.has_w;
+        const bool cw = Tableau::rotation_changes_weight(ALG, W, P.n_units, g.data());
+        if (P.has_w && cw && P.has_floor) {  // the effective cutoff depends on the live count here
+          u64 n = 0;
+          if (int rc = need_n(&n)) return rc;
+          if (n < P.floor_terms) eff_w = false;
         }
         if (!eff_w || !cw) {
-          frame.compose(Tableau::for_rotation(ALG, W, n_units, g.data(), ang));
-          gate_op[gi] = last_op;
+          P.frame.compose(Tableau::for_rotation(ALG, W, P.n_units, g.data(), ang));
+          P.gate_op[gi] = P.last_op;
           continue;
         }
       }
-      const int sign = frame.conjugate_generator(g.data(), gc.data());
-      pq::GateDesc<W> gd;
-      gd.g = make_gen<W>(ALG, gc.data(), sign);
-      gd.sn = std::sin(ang);
-      gd.cs = std::cos(ang);
+      const int sign = P.frame.conjugate_generator(g.data(), gc.data());
+      const double sn = std::sin(ang), cs = std::cos(ang);
+      with_words(W, [&](auto w) {
+        constexpr int WW = decltype(w)::value;
+        pq::GateDesc<WW> gd;
+        gd.g = make_gen<WW>(ALG, gc.data(), sign);
+        gd.sn = sn;
+        gd.cs = cs;
+        const size_t off = P.gdesc.size();
+        P.gdesc.resize(off + sizeof gd / 8);
+        std::memcpy(&P.gdesc[off], &gd, sizeof gd);
+        return 0;
+      });
       pq::OpDesc od;
-      od.kind = std::fabs(gd.sn) < EPS_CLASSIFY ? pq::OP_PHASE : pq::OP_GATE;
-      od.idx = (u32)gdesc.size();
-      gdesc.push_back(gd);
-      ops.push_back(od);
-      last_op = (long)ops.size() - 1;
-      gate_op[gi] = last_op;
+      od.kind = std::fabs(sn) < EPS_CLASSIFY ? pq::OP_PHASE : pq::OP_GATE;
+      od.idx = (u32)P.n_gdesc++;
+      P.ops.push_back(od);
+      P.last_op = (long)P.ops.size() - 1;
+      P.gate_op[gi] = P.last_op;
     }
   }
-  if (int rc = flush()) return rc;
-  if (!began) cudaEventRecord(E->ev_begin, E->stream);
-  const u64 n_fin = n_live;
+  return PQ_OK;
+}
 
-  std::vector<u64> hist(ops.size()), anti(ops.size()), stamps(ops.size());
-  if (!ops.empty()) {
-    cudaMemcpyAsync(hist.data(), E->hist, ops.size() * 8, cudaMemcpyDeviceToHost, E->stream);
-    cudaMemcpyAsync(anti.data(), E->anti, ops.size() * 8, cudaMemcpyDeviceToHost, E->stream);
-    cudaMemcpyAsync(stamps.data(), E->stamps, ops.size() * 8, cudaMemcpyDeviceToHost, E->stream);
+// Enqueues the upload of the ops and gate descriptors not yet on the device.
+void upload_ops(pq_engine* E, Slot& S, Plan& P) {
+  if (P.ops.size() > P.uploaded_ops) {
+    cudaMemcpyAsync(S.d_ops + P.uploaded_ops, P.ops.data() + P.uploaded_ops,
+                    (P.ops.size() - P.uploaded_ops) * sizeof(pq::OpDesc), cudaMemcpyHostToDevice, E->stream);
+    P.uploaded_ops = P.ops.size();
   }
+  if (P.gdesc.size() > P.uploaded_gdesc) {
+    cudaMemcpyAsync(reinterpret_cast<u64*>(S.d_gates) + P.uploaded_gdesc, P.gdesc.data() + P.uploaded_gdesc,
+                    (P.gdesc.size() - P.uploaded_gdesc) * 8, cudaMemcpyHostToDevice, E->stream);
+    P.uploaded_gdesc = P.gdesc.size();
+  }
+}
 
-  // Expectation value and the below-cutoff count.
-  res->expectation_value = 0;
-  res->terms_below_cutoff = 0;
-  u64* d_img = nullptr;
-  int* d_sgn = nullptr;
-  struct FrameFree {
-    u64** a;
-    int** b;
-    ~FrameFree() {
-      if (*a) cudaFree(*a);
-      if (*b) cudaFree(*b);
+pq::SweepArgs sweep_args(Slot& S, const Plan& P, pq::SweepState* st, u32 blk_begin, u32 blk_count) {
+  pq::SweepArgs a{};
+  a.ops = S.d_ops;
+  a.gates = S.d_gates;
+  a.tables = S.d_tables;
+  a.table_len = (u32)P.tlen;
+  a.n_units = P.n_units;
+  a.n_words = (u32)P.W;
+  a.op_begin = (u32)P.done;
+  a.op_end = (u32)P.ops.size();
+  a.cur0 = (u32)S.cur;
+  a.epoch_base = S.epoch_base;
+  a.max_weight = P.wcut;
+  a.has_min_coeff = P.has_c;
+  a.min_coeff = P.ccut;
+  a.min_terms = P.floor_terms;
+  for (int i = 0; i < 2; ++i) {
+    a.keys[i] = S.keys[i];
+    a.coeffs[i] = S.coeffs[i];
+  }
+  a.table = S.table;
+  a.table_mask = S.tcap - 1;
+  a.cap = S.cap;
+  a.status = S.status;
+  a.tickets = S.tickets;
+  a.hist = S.hist;
+  a.anti = S.anti;
+  a.stamps = S.stamps;
+  a.st = st;
+  a.blk_begin = blk_begin;
+  a.blk_count = blk_count;
+  return a;
+}
+
+pq::SweepState fresh_state(const Plan& P) {
+  pq::SweepState s{};
+  s.n[P.done & 1] = P.n_live;
+  s.peak = P.peak;
+  s.halt = pq::NOT_HALTED;
+  return s;
+}
+
+// Reads a plan's sweep state after a launch; on a capacity halt grows its rows
+// (the gate at `done` needs 2 N rows) so that the next launch resumes there.
+int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
+  if (h.error & pq::ERR_BARRIER_TIMEOUT)
+    return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a grid barrier wait expired on the device");
+  if (h.error & pq::ERR_LOOKBACK_TIMEOUT)
+    return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a tile's look-back wait expired on the device");
+  if (h.error) return E->fail(PQ_ERR_CUDA, "device reported error bits " + std::to_string(h.error));
+  S.cur = (int)h.cur;
+  S.epoch_base += (u32)P.ops.size() + 1;
+  P.done = h.end_op;
+  P.n_live = h.n[P.done & 1];
+  P.peak = std::max(P.peak, h.peak);
+  ++P.sweep_launches;
+  if (h.halt != pq::NOT_HALTED) {
+    u64 ncap = next_pow2(std::max<u64>(4 * P.n_live, 2 * S.cap));
+    if (ncap > MAX_ROWS) ncap = MAX_ROWS;
+    if (2 * P.n_live > ncap)
+      return E->fail(PQ_ERR_CEILING, "term index ceiling reached: " + std::to_string(2 * P.n_live) +
+                                         " rows would exceed the engine's capacity");
+    int rc = E->resize(S, ncap, P.n_live, S.cur, P.W);
+    if (rc == PQ_ERR_OOM) rc = E->resize(S, next_pow2(2 * P.n_live), P.n_live, S.cur, P.W);
+    if (rc) return rc;
+  }
+  return PQ_OK;
+}
+
+// Runs every built op of one plan on the whole grid, relaunching after
+// capacity growth.
+int execute_single(pq_engine* E, Slot& S, Plan& P, int grid, bool* began) {
+  cudaError_t e;
+  upload_ops(E, S, P);
+  while (P.done < P.ops.size()) {
+    E->h_states[0] = fresh_state(P);
+    cudaMemcpyAsync(E->d_states, E->h_states, sizeof(pq::SweepState), cudaMemcpyHostToDevice, E->stream);
+    cudaMemsetAsync(S.tickets + P.done, 0, (P.ops.size() - P.done) * 4, E->stream);
+    const pq::SweepArgs a = sweep_args(S, P, E->d_states, 0, (u32)grid);
+    if (!*began) {  // device time starts at the first sweep
+      cudaEventRecord(E->ev_begin, E->stream);
+      *began = true;
     }
-  } ff{&d_img, &d_sgn};
-  if (!frame.identity) {
-    if ((e = cudaMalloc(&d_img, frame.rd_img.size() * 8)) != cudaSuccess) return E->cuda_fail(e, "frame");
-    if ((e = cudaMalloc(&d_sgn, frame.rd_sign.size() * sizeof(int))) != cudaSuccess) return E->cuda_fail(e, "frame");
-    cudaMemcpyAsync(d_img, frame.rd_img.data(), frame.rd_img.size() * 8, cudaMemcpyHostToDevice, E->stream);
-    cudaMemcpyAsync(d_sgn, frame.rd_sign.data(), frame.rd_sign.size() * sizeof(int), cudaMemcpyHostToDevice,
-                    E->stream);
+    cudaEventRecord(E->ev_l0, E->stream);
+    e = with_words(P.W, [&](auto w) {
+      constexpr int WW = decltype(w)::value;
+      return P.alg == 0 ? pq::launch_sweep<WW, 0>(a, grid, E->stream) : pq::launch_sweep<WW, 1>(a, grid, E->stream);
+    });
+    if (e != cudaSuccess) return E->cuda_fail(e, "sweep launch");
+    cudaEventRecord(E->ev_l1, E->stream);
+    ++E->launches;
+    cudaMemcpyAsync(E->h_states, E->d_states, sizeof(pq::SweepState), cudaMemcpyDeviceToHost, E->stream);
+    if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "sweep");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, E->ev_l0, E->ev_l1);
+    P.sweep_ms += ms;
+    if (int rc = absorb_state(E, S, P, E->h_states[0])) return rc;
   }
-  if (diag || has_c) {
+  return PQ_OK;
+}
+
+// Enqueues the expectation value and the final-term readout of one plan.
+int finalize(pq_engine* E, Slot& S, Plan& P, std::vector<pq::ExpectPartial>* parts) {
+  cudaError_t e;
+  const Inputs& in = *P.in;
+  const int W = P.W, ALG = P.alg;
+  const u64 n_fin = P.n_live;
+  if (!P.frame.identity) {
+    const size_t ni = P.frame.rd_img.size(), ns = P.frame.rd_sign.size();
+    if (S.frame_cap < ni) {
+      if (S.frame_img) cudaFree(S.frame_img);
+      if (S.frame_sgn) cudaFree(S.frame_sgn);
+      S.frame_img = nullptr;
+      S.frame_sgn = nullptr;
+      S.frame_cap = 0;
+      if ((e = cudaMalloc(&S.frame_img, ni * 8)) != cudaSuccess) return E->cuda_fail(e, "frame");
+      if ((e = cudaMalloc(&S.frame_sgn, ni * sizeof(int))) != cudaSuccess) return E->cuda_fail(e, "frame");
+      S.frame_cap = ni;
+    }
+    cudaMemcpyAsync(S.frame_img, P.frame.rd_img.data(), ni * 8, cudaMemcpyHostToDevice, E->stream);
+    cudaMemcpyAsync(S.frame_sgn, P.frame.rd_sign.data(), ns * sizeof(int), cudaMemcpyHostToDevice, E->stream);
+  }
+  const u64* d_img = P.frame.identity ? nullptr : S.frame_img;
+  const int* d_sgn = P.frame.identity ? nullptr : S.frame_sgn;
+  parts->clear();
+  if (in.diag || P.has_c) {
     pq::ExpectArgs xa{};
-    if (diag) {
-      for (u32 u = 0; u < n_units; ++u) {
-        const u64 bit = (u / 64 < nd) ? (diag[u / 64] >> (u % 64)) & 1 : 0;
+    if (in.diag) {
+      for (u32 u = 0; u < P.n_units; ++u) {
+        const u64 bit = (u / 64 < in.nd) ? (in.diag[u / 64] >> (u % 64)) & 1 : 0;
         if (!bit) continue;
         const u32 pos = ALG == 0 ? 2 * u + 1 : 2 * u;
         if (pos / 64 < (u32)W) xa.state[pos / 64] |= 1ULL << (pos % 64);
       }
     }
-    xa.n_units = n_units;
-    xa.has_min_coeff = has_c;
-    xa.min_coeff = ccut;
+    xa.n_units = P.n_units;
+    xa.has_min_coeff = P.has_c;
+    xa.min_coeff = P.ccut;
     xa.frame_images = d_img;
     xa.frame_signs = d_sgn;
-    xa.frame_rows = (u32)frame.rows;
+    xa.frame_rows = (u32)P.frame.rows;
     ++E->launches;
-    if ((e = pq::launch_expect<W, ALG>(xa, E->keys[E->cur], E->coeffs[E->cur], n_fin, E->partials, E->expect_grid,
-                                       E->stream)) != cudaSuccess)
-      return E->cuda_fail(e, "expectation launch");
-    cudaEventRecord(E->ev_end, E->stream);
-    std::vector<pq::ExpectPartial> parts(E->expect_grid);
-    cudaMemcpyAsync(parts.data(), E->partials, parts.size() * sizeof(pq::ExpectPartial), cudaMemcpyDeviceToHost,
+    e = with_words(W, [&](auto w) {
+      constexpr int WW = decltype(w)::value;
+      return ALG == 0 ? pq::launch_expect<WW, 0>(xa, S.keys[S.cur], S.coeffs[S.cur], n_fin, S.partials,
+                                                  E->expect_grid, E->stream)
+                      : pq::launch_expect<WW, 1>(xa, S.keys[S.cur], S.coeffs[S.cur], n_fin, S.partials,
+                                                  E->expect_grid, E->stream);
+    });
+    if (e != cudaSuccess) return E->cuda_fail(e, "expectation launch");
+    parts->resize(E->expect_grid);
+    cudaMemcpyAsync(parts->data(), S.partials, parts->size() * sizeof(pq::ExpectPartial), cudaMemcpyDeviceToHost,
                     E->stream);
-    if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "expectation");
+  }
+  S.out_keys.clear();
+  S.out_coeffs.clear();
+  S.out_words = in.in_words;
+  if (in.cfg->want_terms && n_fin) {
+    S.out_keys.resize(n_fin * W);
+    S.out_coeffs.resize(n_fin);
+    int src = S.cur;
+    if (!P.frame.identity) {  // the alternate buffer is free after the sweep: conjugate into it
+      src = S.cur ^ 1;
+      ++E->launches;
+      with_words(W, [&](auto w) {
+        pq::launch_conjugate<decltype(w)::value>(S.keys[S.cur], S.coeffs[S.cur], n_fin, d_img, d_sgn,
+                                                 (u32)P.frame.rows, ALG, S.keys[src], S.coeffs[src], E->stream);
+        return 0;
+      });
+    }
+    cudaMemcpyAsync(S.out_keys.data(), S.keys[src], n_fin * W * 8, cudaMemcpyDeviceToHost, E->stream);
+    cudaMemcpyAsync(S.out_coeffs.data(), S.coeffs[src], n_fin * 8, cudaMemcpyDeviceToHost, E->stream);
+  }
+  return PQ_OK;
+}
+
+// Host half of the result, once the stream has drained: the double-double
+// sum of the partials, per-gate live counts and the per-kind totals (inputs
+// of the algorithmic-bytes roofline, and the device-clock split of the sweep).
+int finish(pq_engine* E, Slot& S, Plan& P, const std::vector<pq::ExpectPartial>& parts) {
+  const Inputs& in = *P.in;
+  pq_result* res = in.res;
+  if (!parts.empty()) {
     double hi = 0, lo = 0;
     auto dd = [&](double v) {
       const double s = hi + v, bb = s - hi;
@@ -817,42 +1019,29 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
       dd(p.lo);
       below += p.below;
     }
-    if (diag) res->expectation_value = hi + lo;
-    res->terms_below_cutoff = has_c ? below : 0;
-  } else {
-    cudaEventRecord(E->ev_end, E->stream);
-    if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "sync");
+    if (in.diag) res->expectation_value = hi + lo;
+    res->terms_below_cutoff = P.has_c ? below : 0;
   }
-
-  if (n_terms_out)
-    for (size_t gi = 0; gi < n_gates; ++gi) n_terms_out[gi] = gate_op[gi] >= 0 ? hist[gate_op[gi]] : n0;
-
-  E->out_keys.clear();
-  E->out_coeffs.clear();
-  if (cfg->want_terms && n_fin) {
-    E->out_keys.resize(n_fin * W);
-    E->out_coeffs.resize(n_fin);
-    if (frame.identity) {
-      cudaMemcpyAsync(E->out_keys.data(), E->keys[E->cur], n_fin * W * 8, cudaMemcpyDeviceToHost, E->stream);
-      cudaMemcpyAsync(E->out_coeffs.data(), E->coeffs[E->cur], n_fin * 8, cudaMemcpyDeviceToHost, E->stream);
-    } else {
-      // The alternate buffer is free after the sweep: conjugate into it.
-      const int alt = E->cur ^ 1;
-      ++E->launches;
-      pq::launch_conjugate<W>(E->keys[E->cur], E->coeffs[E->cur], n_fin, d_img, d_sgn, (u32)frame.rows, ALG,
-                              E->keys[alt], E->coeffs[alt], E->stream);
-      cudaMemcpyAsync(E->out_keys.data(), E->keys[alt], n_fin * W * 8, cudaMemcpyDeviceToHost, E->stream);
-      cudaMemcpyAsync(E->out_coeffs.data(), E->coeffs[alt], n_fin * 8, cudaMemcpyDeviceToHost, E->stream);
-    }
-    if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "terms copy");
+  if (S.out_words < P.W && !S.out_coeffs.empty()) {  // drop the zero words the device width added
+    const size_t n = S.out_coeffs.size();
+    for (size_t i = 0; i < n; ++i)
+      for (int w = 0; w < S.out_words; ++w) S.out_keys[i * S.out_words + w] = S.out_keys[i * P.W + w];
+    S.out_keys.resize(n * S.out_words);
   }
-
-  // Per-kind totals (inputs of the algorithmic-bytes roofline) and the
-  // device-clock split of the sweep time by op kind.
-  for (size_t i = 0; i < ops.size(); ++i) {
-    const u64 n_in = i ? hist[i - 1] : n0;
+  const size_t no = P.ops.size();
+  std::vector<u64> hist(no), anti(no), stamps(no);
+  if (no) {
+    cudaMemcpyAsync(hist.data(), S.hist, no * 8, cudaMemcpyDeviceToHost, E->stream);
+    cudaMemcpyAsync(anti.data(), S.anti, no * 8, cudaMemcpyDeviceToHost, E->stream);
+    cudaMemcpyAsync(stamps.data(), S.stamps, no * 8, cudaMemcpyDeviceToHost, E->stream);
+    if (cudaError_t e = cudaStreamSynchronize(E->stream)) return E->cuda_fail(e, "op statistics");
+  }
+  if (in.n_terms_out)
+    for (size_t g = 0; g < in.n_gates; ++g) in.n_terms_out[g] = P.gate_op[g] >= 0 ? hist[P.gate_op[g]] : P.n0;
+  for (size_t i = 0; i < no; ++i) {
+    const u64 n_in = i ? hist[i - 1] : P.n0;
     const double op_ms = i ? (double)(stamps[i] - stamps[i - 1]) * 1e-6 : 0.0;
-    switch (ops[i].kind) {
+    switch (P.ops[i].kind) {
       case pq::OP_GATE:
         ++res->gate_ops;
         res->gate_ms += op_ms;
@@ -869,28 +1058,170 @@ int run_impl(pq_engine* E, const pq_run_config* cfg, const u64* obs_words, const
         ++res->noise_ops;
         res->noise_ms += op_ms;
         res->sum_rows_noise += n_in;
-        res->sum_kept += ops[i].kind == pq::OP_NOISE_COMPACT ? hist[i] : 0;
+        res->sum_kept += P.ops[i].kind == pq::OP_NOISE_COMPACT ? hist[i] : 0;
     }
   }
-  float ms = 0;
-  cudaEventElapsedTime(&ms, E->ev_begin, E->ev_end);
-  res->device_ms = ms;
-  res->sweep_ms = sweep_ms;
-  res->sweep_launches = sweep_launches;
-  res->n_final = n_fin;
-  res->peak_terms = peak;
-  res->sparse_key_bytes = n_fin * W * 8 + E->tcap * 8;
-  res->n_layers_run = n_layers;
-  res->n_gates_run = n_gates;
+  res->sweep_ms = P.sweep_ms;
+  res->sweep_launches = P.sweep_launches;
+  res->n_final = P.n_live;
+  res->peak_terms = P.peak;
+  res->sparse_key_bytes = P.n_live * P.W * 8 + S.tcap * 8;
+  res->n_layers_run = in.n_layers;
+  res->n_gates_run = in.n_gates;
   return PQ_OK;
 }
 
-template <int W>
-int run_alg(pq_engine* E, const pq_run_config* c, const u64* ow, const double* oc, size_t no, const u64* gw,
-            const double* ga, size_t ng, const u32* lo, size_t nl, const u64* d, size_t nd, u64* nt,
-            pq_result* r) {
-  if (c->basis_kind == PQ_BASIS_PAULI) return run_impl<W, 0>(E, c, ow, oc, no, gw, ga, ng, lo, nl, d, nd, nt, r);
-  return run_impl<W, 1>(E, c, ow, oc, no, gw, ga, ng, lo, nl, d, nd, nt, r);
+int run_one(pq_engine* E, const Inputs& in, int W) {
+  if (int rc = E->ensure_slots(1)) return rc;
+  Slot& S = E->slots[0];
+  Plan P;
+  if (int rc = prepare(E, P, in, W)) return rc;
+  if (int rc = setup_slot(E, S, P)) return rc;
+  const int grid = with_words(W, [&](auto w) {
+    constexpr int WW = decltype(w)::value;
+    return P.alg == 0 ? pq::sweep_grid<WW, 0>((int)in.cfg->blocks_per_sm)
+                      : pq::sweep_grid<WW, 1>((int)in.cfg->blocks_per_sm);
+  });
+  bool began = false;
+  auto need_n = [&](u64* n) -> int {
+    if (int rc = execute_single(E, S, P, grid, &began)) return rc;
+    *n = P.n_live;
+    return PQ_OK;
+  };
+  if (int rc = build_ops(P, need_n)) return rc;
+  if (int rc = execute_single(E, S, P, grid, &began)) return rc;
+  if (!began) cudaEventRecord(E->ev_begin, E->stream);
+  std::vector<pq::ExpectPartial> parts;
+  if (int rc = finalize(E, S, P, &parts)) return rc;
+  cudaEventRecord(E->ev_end, E->stream);
+  if (cudaError_t e = cudaStreamSynchronize(E->stream)) return E->cuda_fail(e, "finalize");
+  if (int rc = finish(E, S, P, parts)) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, E->ev_begin, E->ev_end);
+  in.res->device_ms = ms;
+  return PQ_OK;
+}
+
+// Splits `blocks` among the instances in `todo`: one each, the rest equally
+// (split 0) or in proportion to remaining ops x (live terms + units), the work
+// still ahead if the live count stayed where it is (split 1).
+std::vector<u32> share_blocks(const std::vector<Plan>& plans, const std::vector<size_t>& todo, size_t blocks,
+                              u32 split) {
+  std::vector<double> wgt(todo.size(), 1.0);
+  if (split == 1)
+    for (size_t k = 0; k < todo.size(); ++k) {
+      const Plan& P = plans[todo[k]];
+      wgt[k] = (double)(P.ops.size() - P.done) * ((double)P.n_live + (double)P.n_units);
+    }
+  double wsum = 0;
+  for (double w : wgt) wsum += w;
+  std::vector<u32> cnt(todo.size(), 1);
+  const size_t spare = blocks - todo.size();
+  size_t given = 0;
+  for (size_t k = 0; k < todo.size() && wsum > 0; ++k) {
+    const u32 extra = (u32)std::floor((double)spare * wgt[k] / wsum);
+    cnt[k] += extra;
+    given += extra;
+  }
+  for (size_t k = 0; given < spare; k = (k + 1) % todo.size(), ++given) ++cnt[k];
+  return cnt;
+}
+
+// A batch in cooperative launches of batch_sweep_kernel: every unfinished
+// instance gets a contiguous slice of the grid (at least one block) and runs
+// its own op sequence with its own barrier.  When rebalance_pct of the grid
+// has been left by instances that finished (or stopped for capacity), the
+// rest stop at their next op boundary and the next launch re-splits the whole
+// grid among the instances still running; instances that halted for capacity
+// are grown first.
+int run_batch(pq_engine* E, const std::vector<Inputs>& ins, int WM, const pq_batch_tuning& tune) {
+  const size_t n = ins.size();
+  const int alg = (int)ins[0].cfg->basis_kind;
+  if (int rc = E->ensure_slots(n)) return rc;
+  std::vector<Plan> plans(n);
+  auto no_sync = [&](u64*) -> int {
+    return E->fail(PQ_ERR_UNSUPPORTED,
+                   "a batch cannot decide Clifford deferral under a TermBudget floor with a weight cut; run that "
+                   "instance with pq_run");
+  };
+  for (size_t i = 0; i < n; ++i) {
+    const int W = std::max(ins[i].in_words, WM > 1 ? WM / 2 : 1);
+    if (int rc = prepare(E, plans[i], ins[i], W)) return rc;
+    if (int rc = setup_slot(E, E->slots[i], plans[i])) return rc;
+    if (int rc = build_ops(plans[i], no_sync)) return rc;
+    upload_ops(E, E->slots[i], plans[i]);
+  }
+  const int grid_max = with_words(WM, [&](auto w) {
+    constexpr int WW = decltype(w)::value;
+    return alg == 0 ? pq::batch_grid<WW, 0>((int)tune.blocks_per_sm) : pq::batch_grid<WW, 1>((int)tune.blocks_per_sm);
+  });
+  if (int rc = E->ensure_batch_arrays(n, (size_t)grid_max)) return rc;
+  cudaError_t e;
+  bool began = false;
+  double sweep_ms = 0;
+  std::vector<size_t> todo;
+  for (;;) {
+    todo.clear();
+    for (size_t i = 0; i < n && todo.size() < (size_t)grid_max; ++i)
+      if (plans[i].done < plans[i].ops.size()) todo.push_back(i);
+    if (todo.empty()) break;
+    const std::vector<u32> cnt = share_blocks(plans, todo, (size_t)grid_max, tune.split);
+    // One instance left: nothing to re-split.
+    const bool rebalance = tune.rebalance_pct > 0 && todo.size() > 1;
+    const u32 yield_at = std::max<u32>(1, (u32)((u64)grid_max * std::min<u32>(tune.rebalance_pct, 100) / 100));
+    u32 off = 0;
+    for (size_t k = 0; k < todo.size(); ++k) {
+      Slot& S = E->slots[todo[k]];
+      Plan& P = plans[todo[k]];
+      E->h_states[k] = fresh_state(P);
+      cudaMemsetAsync(S.tickets + P.done, 0, (P.ops.size() - P.done) * 4, E->stream);
+      E->h_args[k] = sweep_args(S, P, E->d_states + k, off, cnt[k]);
+      E->h_args[k].idle_blocks = rebalance ? E->d_idle : nullptr;
+      E->h_args[k].yield_at = yield_at;
+      for (u32 b = 0; b < cnt[k]; ++b) E->h_block_inst[off + b] = (u32)k;
+      off += cnt[k];
+    }
+    cudaMemcpyAsync(E->d_states, E->h_states, todo.size() * sizeof(pq::SweepState), cudaMemcpyHostToDevice,
+                    E->stream);
+    cudaMemcpyAsync(E->d_args, E->h_args, todo.size() * sizeof(pq::SweepArgs), cudaMemcpyHostToDevice, E->stream);
+    cudaMemcpyAsync(E->d_block_inst, E->h_block_inst, off * 4, cudaMemcpyHostToDevice, E->stream);
+    cudaMemsetAsync(E->d_idle, 0, sizeof(u32), E->stream);
+    if (!began) {
+      cudaEventRecord(E->ev_begin, E->stream);
+      began = true;
+    }
+    cudaEventRecord(E->ev_l0, E->stream);
+    e = with_words(WM, [&](auto w) {
+      constexpr int WW = decltype(w)::value;
+      return alg == 0 ? pq::launch_batch_sweep<WW, 0>(E->d_args, E->d_block_inst, (int)off, E->stream)
+                      : pq::launch_batch_sweep<WW, 1>(E->d_args, E->d_block_inst, (int)off, E->stream);
+    });
+    if (e != cudaSuccess) return E->cuda_fail(e, "batch sweep launch");
+    cudaEventRecord(E->ev_l1, E->stream);
+    ++E->launches;
+    cudaMemcpyAsync(E->h_states, E->d_states, todo.size() * sizeof(pq::SweepState), cudaMemcpyDeviceToHost,
+                    E->stream);
+    if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "batch sweep");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, E->ev_l0, E->ev_l1);
+    sweep_ms += ms;
+    for (size_t k = 0; k < todo.size(); ++k)
+      if (int rc = absorb_state(E, E->slots[todo[k]], plans[todo[k]], E->h_states[k])) return rc;
+  }
+  if (!began) cudaEventRecord(E->ev_begin, E->stream);
+  std::vector<std::vector<pq::ExpectPartial>> parts(n);
+  for (size_t i = 0; i < n; ++i)
+    if (int rc = finalize(E, E->slots[i], plans[i], &parts[i])) return rc;
+  cudaEventRecord(E->ev_end, E->stream);
+  if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "finalize");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, E->ev_begin, E->ev_end);
+  for (size_t i = 0; i < n; ++i) {
+    if (int rc = finish(E, E->slots[i], plans[i], parts[i])) return rc;
+    ins[i].res->device_ms = ms;  // the batch's device time
+    ins[i].res->sweep_ms = sweep_ms;
+  }
+  return PQ_OK;
 }
 
 }  // namespace
@@ -919,15 +1250,14 @@ int pq_engine_create(pq_engine** out, int device) {
   if (!coop) return PQ_ERR_CUDA;
   E->device = device;
   if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess) return PQ_ERR_CUDA;
-  if (cudaMalloc(&E->st, sizeof(pq::SweepState)) != cudaSuccess) return PQ_ERR_OOM;
-  if (cudaMallocHost(&E->h_st, sizeof(pq::SweepState)) != cudaSuccess) return PQ_ERR_OOM;
   if (cudaMalloc(&E->d_err, sizeof(u32)) != cudaSuccess) return PQ_ERR_OOM;
+  if (cudaMalloc(&E->d_idle, sizeof(u32)) != cudaSuccess) return PQ_ERR_OOM;
   cudaMemset(E->d_err, 0, sizeof(u32));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   E->expect_grid = 4 * sms;
-  if (cudaMalloc(&E->partials, sizeof(pq::ExpectPartial) * E->expect_grid) != cudaSuccess) return PQ_ERR_OOM;
   for (cudaEvent_t* ev : {&E->ev_begin, &E->ev_end, &E->ev_l0, &E->ev_l1}) cudaEventCreate(ev);
+  if (E->ensure_slots(1) != PQ_OK) return PQ_ERR_OOM;
   *out = E.release();
   return PQ_OK;
 }
@@ -935,47 +1265,94 @@ int pq_engine_create(pq_engine** out, int device) {
 void pq_engine_destroy(pq_engine* E) { delete E; }
 const char* pq_engine_last_error(const pq_engine* E) { return E ? E->err.c_str() : "null engine"; }
 
+}  // extern "C"
+
+namespace {
+
+// Argument checks shared by pq_run and pq_run_batch; sets the key width.
+int check_inputs(pq_engine* E, const pq_run_config* cfg, size_t ng, const uint32_t* lo, size_t nl, int* W_out) {
+  if (cfg->basis_kind > 1) return E->fail(PQ_ERR_INVALID, "basis_kind must be 0 (Pauli) or 1 (Majorana)");
+  const uint32_t W = pq_words_for_units(cfg->n_units);
+  if (!W)
+    return E->fail(PQ_ERR_INVALID, "propaq: " + std::to_string(cfg->n_units) +
+                                       " units exceeds the engine's maximum of 2048");
+  if (W > 8)
+    return E->fail(PQ_ERR_UNSUPPORTED, "registers wider than 256 units (" + std::to_string(W) +
+                                           " words) are not compiled into this build");
+  if (nl && (!lo || lo[0] != 0 || lo[nl] != ng)) return E->fail(PQ_ERR_INVALID, "layer offsets do not cover the gates");
+  if (!nl && ng) return E->fail(PQ_ERR_INVALID, "layer offsets do not cover the gates");
+  for (size_t l = 0; l < nl; ++l)
+    if (lo[l + 1] < lo[l]) return E->fail(PQ_ERR_INVALID, "layer offsets must be non-decreasing");
+  *W_out = (int)W;
+  return PQ_OK;
+}
+
+// uint64_t and the kernels' unsigned long long are both 64-bit words.
+inline const u64* K(const uint64_t* p) { return reinterpret_cast<const u64*>(p); }
+
+}  // namespace
+
+extern "C" {
+
 int pq_run(pq_engine* E, const pq_run_config* cfg, const uint64_t* ow, const double* oc, size_t no,
            const uint64_t* gw, const double* ga, size_t ng, const uint32_t* lo, size_t nl, const uint64_t* d,
            size_t nd, uint64_t* nt, pq_result* r) {
   if (!E || !cfg || !r) return PQ_ERR_INVALID;
   std::memset(r, 0, sizeof(*r));
   E->err.clear();
-  if (cfg->basis_kind > 1) return E->fail(PQ_ERR_INVALID, "basis_kind must be 0 (Pauli) or 1 (Majorana)");
-  const uint32_t W = pq_words_for_units(cfg->n_units);
-  if (!W)
-    return E->fail(PQ_ERR_INVALID, "propaq: " + std::to_string(cfg->n_units) +
-                                       " units exceeds the engine's maximum of 2048");
-  if (nl && (!lo || lo[0] != 0 || lo[nl] != ng)) return E->fail(PQ_ERR_INVALID, "layer offsets do not cover the gates");
-  for (size_t l = 0; l < nl; ++l)
-    if (lo[l + 1] < lo[l]) return E->fail(PQ_ERR_INVALID, "layer offsets must be non-decreasing");
+  int W = 0;
+  if (int rc = check_inputs(E, cfg, ng, lo, nl, &W)) return rc;
   if (cudaSetDevice(E->device) != cudaSuccess) return E->fail(PQ_ERR_CUDA, "cudaSetDevice failed");
   const u64 l0 = E->launches;
-  // uint64_t and the kernels' unsigned long long are both 64-bit words.
-  auto K = [](const uint64_t* p) { return reinterpret_cast<const u64*>(p); };
-  auto Kw = reinterpret_cast<u64*>(nt);
-  int rc;
-  switch (W) {
-    case 1: rc = run_alg<1>(E, cfg, K(ow), oc, no, K(gw), ga, ng, lo, nl, K(d), nd, Kw, r); break;
-    case 2: rc = run_alg<2>(E, cfg, K(ow), oc, no, K(gw), ga, ng, lo, nl, K(d), nd, Kw, r); break;
-    case 4: rc = run_alg<4>(E, cfg, K(ow), oc, no, K(gw), ga, ng, lo, nl, K(d), nd, Kw, r); break;
-    case 8: rc = run_alg<8>(E, cfg, K(ow), oc, no, K(gw), ga, ng, lo, nl, K(d), nd, Kw, r); break;
-    default:
-      rc = E->fail(PQ_ERR_UNSUPPORTED, "registers wider than 256 units (" + std::to_string(W) +
-                                           " words) are not compiled into this build");
-  }
+  const Inputs in{cfg, K(ow), oc, no, K(gw), ga, ng, lo, nl, K(d), nd, reinterpret_cast<u64*>(nt), r, W};
+  const int rc = run_one(E, in, W);
   r->gpu_launches = E->launches - l0;
   return rc;
 }
 
-size_t pq_result_terms(pq_engine* E, uint64_t* keys, double* coeffs, size_t cap) {
-  const size_t n = E->out_coeffs.size();
+int pq_run_batch(pq_engine* E, const pq_instance* insts, size_t n, const pq_batch_tuning* tuning) {
+  if (!E || !insts || !n) return PQ_ERR_INVALID;
+  E->err.clear();
+  const pq_batch_tuning tune = tuning ? *tuning : pq_batch_tuning{0, 1, 25};
+  if (tune.split > 1) return E->fail(PQ_ERR_INVALID, "split must be 0 (equal) or 1 (by remaining work)");
+  if (tune.rebalance_pct > 100) return E->fail(PQ_ERR_INVALID, "rebalance_pct must be 0..100");
+  const uint32_t basis = insts[0].cfg.basis_kind;
+  int WM = 1;
+  std::vector<Inputs> ins(n);
+  for (size_t i = 0; i < n; ++i) {
+    const pq_instance& x = insts[i];
+    if (!x.result) return E->fail(PQ_ERR_INVALID, "instance " + std::to_string(i) + " has no result");
+    std::memset(x.result, 0, sizeof(pq_result));
+    if (x.cfg.basis_kind != basis) return E->fail(PQ_ERR_INVALID, "a batch mixes Pauli and Majorana instances");
+    int W = 0;
+    if (int rc = check_inputs(E, &x.cfg, x.n_gates, x.layer_offsets, x.n_layers, &W)) return rc;
+    WM = std::max(WM, W);
+    ins[i] = Inputs{&x.cfg,          K(x.obs_words),  x.obs_coeffs,  x.n_obs,
+                    K(x.gate_words), x.gate_angles,   x.n_gates,     x.layer_offsets,
+                    x.n_layers,      K(x.diag_state), x.diag_words,  reinterpret_cast<u64*>(x.n_terms_out),
+                    x.result,        W};
+  }
+  if (cudaSetDevice(E->device) != cudaSuccess) return E->fail(PQ_ERR_CUDA, "cudaSetDevice failed");
+  const u64 l0 = E->launches;
+  const int rc = run_batch(E, ins, WM, tune);
+  for (size_t i = 0; i < n; ++i) insts[i].result->gpu_launches = E->launches - l0;
+  return rc;
+}
+
+size_t pq_result_terms_at(pq_engine* E, size_t index, uint64_t* keys, double* coeffs, size_t cap) {
+  if (!E || index >= E->slots.size()) return 0;
+  const Slot& S = E->slots[index];
+  const size_t n = S.out_coeffs.size();
   const size_t m = std::min(n, cap);
-  if (m && E->W) {
-    std::memcpy(keys, E->out_keys.data(), m * E->W * 8);
-    std::memcpy(coeffs, E->out_coeffs.data(), m * 8);
+  if (m) {
+    std::memcpy(keys, S.out_keys.data(), m * S.out_words * 8);
+    std::memcpy(coeffs, S.out_coeffs.data(), m * 8);
   }
   return n;
+}
+
+size_t pq_result_terms(pq_engine* E, uint64_t* keys, double* coeffs, size_t cap) {
+  return pq_result_terms_at(E, 0, keys, coeffs, cap);
 }
 
 int pq_plugin_load_noise(const char* path, const char* cfg, pq_plugin** out, char* err, size_t n) {

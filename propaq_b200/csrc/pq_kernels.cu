@@ -58,18 +58,24 @@ __device__ __forceinline__ u64 pack_status(u32 epoch, u32 flag, u32 value) {
 __device__ __forceinline__ u64 ld_volatile(const u64* p) { return *(const volatile u64*)p; }
 __device__ __forceinline__ void st_volatile(u64* p, u64 v) { *(volatile u64*)p = v; }
 
+// The blocks running one propagation: `bid` of `nblk` (the whole grid for a
+// single run, a contiguous slice of it for one instance of a batch).
+struct Grp {
+  u32 bid, nblk;
+};
+
 // Grid barrier (sense by generation), two-level: each block arrives on one of
 // BAR_GROUPS counters (each on its own 128-byte line), the last arrival of a
 // group arrives on the top counter, and the last top arrival releases
 // everyone by bumping the generation.  Every wait is bounded; once one
 // expires, ERR_BARRIER_TIMEOUT makes every later barrier fall through.
-__device__ __forceinline__ void grid_barrier(SweepState* st, u32& gen) {
+__device__ __forceinline__ void grid_barrier(SweepState* st, u32& gen, const Grp g_) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const u32 g = gen;
-    const u32 nb = gridDim.x;
-    const u32 grp = blockIdx.x % BAR_GROUPS;
+    const u32 nb = g_.nblk;
+    const u32 grp = g_.bid % BAR_GROUPS;
     const u32 in_grp = nb / BAR_GROUPS + (grp < nb % BAR_GROUPS ? 1u : 0u);
     const u32 n_grp = nb < BAR_GROUPS ? nb : BAR_GROUPS;
     bool last = false;
@@ -298,7 +304,7 @@ __device__ __forceinline__ void tile_scan(u32 flags, unsigned* masks, TileSmem& 
 // waits on blocks that are running.
 template <int W, int ALG, int IT>
 __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
-                                           double* coeffs, TileSmem& sm) {
+                                           double* coeffs, TileSmem& sm, const Grp grp) {
   using Ops = typename Alg<ALG>::T;
   constexpr int TL = BLOCK * IT;
   SweepState* st = a.st;
@@ -321,7 +327,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
   };
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u32 n_anti = 0;
-  for (u32 t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (u32 t = grp.bid; t < ntiles; t += grp.nblk) {
     u64 key[IT][W];
     u32 anti = 0;
 #pragma unroll
@@ -510,15 +516,15 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
 
 template <int W, int ALG>
 __device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
-                                        double* coeffs, TileSmem& sm) {
+                                        double* coeffs, TileSmem& sm, const Grp grp) {
   if (N == 0) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(&a.st->n[(op + 1) & 1], 0);
+    if (grp.bid == 0 && threadIdx.x == 0) st_volatile(&a.st->n[(op + 1) & 1], 0);
     return;
   }
   // Few rows: one row per thread and at most one 256-row tile per block, so
   // every row's chain of dependent loads runs at once.
-  if (N <= (u64)gridDim.x * BLOCK)
-    gate_tiles<W, ALG, 1>(a, d, op, N, keys, coeffs, sm);
+  if (N <= (u64)grp.nblk * BLOCK)
+    gate_tiles<W, ALG, 1>(a, d, op, N, keys, coeffs, sm, grp);
   else
     gate_tiles_large<W, ALG>(a, d, op, N, keys, coeffs, sm);
 }
@@ -526,9 +532,9 @@ __device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d
 // A rotation with |sin| < 1e-9 only scales the anticommuting rows by cos
 // (partitioned_termsum.rs:303-308, termsum.rs:551-557).
 template <int W, int ALG>
-__device__ __noinline__ void phase_op(const GateDesc<W>& d, u64 N, const u64* keys, double* coeffs) {
+__device__ __noinline__ void phase_op(const GateDesc<W>& d, u64 N, const u64* keys, double* coeffs, const Grp grp) {
   using Ops = typename Alg<ALG>::T;
-  for (u64 r = (u64)blockIdx.x * BLOCK + threadIdx.x; r < N; r += (u64)gridDim.x * BLOCK) {
+  for (u64 r = (u64)grp.bid * BLOCK + threadIdx.x; r < N; r += (u64)grp.nblk * BLOCK) {
     u64 key[W];
     load_key<W>(keys, r, key);
     if (Ops::template anticommutes<W>(d.g, key)) coeffs[r] = __dmul_rn(__ldcg(coeffs + r), d.cs);
@@ -538,10 +544,10 @@ __device__ __noinline__ void phase_op(const GateDesc<W>& d, u64 N, const u64* ke
 // Noise without truncation: c *= factor[min(w, len-1)] (engine.rs:119-125).
 template <int W, int ALG>
 __device__ __noinline__ void noise_scale_op(const SweepArgs& a, const double* factors, u64 N, const u64* keys,
-                                               double* coeffs) {
+                                               double* coeffs, const Grp grp) {
   using Ops = typename Alg<ALG>::T;
   const u32 last = a.table_len - 1;
-  for (u64 r = (u64)blockIdx.x * BLOCK + threadIdx.x; r < N; r += (u64)gridDim.x * BLOCK) {
+  for (u64 r = (u64)grp.bid * BLOCK + threadIdx.x; r < N; r += (u64)grp.nblk * BLOCK) {
     u64 key[W];
     load_key<W>(keys, r, key);
     const u32 w = Ops::template weight<W>(key, a.n_units);
@@ -555,7 +561,7 @@ __device__ __noinline__ void noise_scale_op(const SweepArgs& a, const double* fa
 template <int W, int ALG>
 __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* factors, u32 op, u64 N,
                                                  const u64* keys, const double* coeffs, u64* keys_out,
-                                                 double* coeffs_out, TileSmem& sm) {
+                                                 double* coeffs_out, TileSmem& sm, const Grp grp) {
   using Ops = typename Alg<ALG>::T;
   constexpr int IT = 1;
   constexpr int TL = BLOCK * IT;
@@ -563,13 +569,13 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
   const u32 ntiles = (u32)((N + TL - 1) / TL);
   u64* n_out = &st->n[(op + 1) & 1];
   if (ntiles == 0) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
+    if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
     return;
   }
   const u32 last = a.table_len - 1;
   const u32 epoch = a.epoch_base + op;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (u32 t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (u32 t = grp.bid; t < ntiles; t += grp.nblk) {
     u32 keep = 0;
     double cv[IT];
     u64 key[IT][W];
@@ -607,8 +613,9 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
   }
 }
 
+// Runs ops [a.op_begin, a.op_end) of one propagation on the blocks of `grp`.
 template <int W, int ALG>
-__global__ void __launch_bounds__(BLOCK, (W >= 8 ? 2 : (W == 4 ? 3 : 4))) sweep_kernel(const SweepArgs a) {
+__device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   __shared__ TileSmem sm;
   __shared__ GateDesc<W> sgate;
   SweepState* st = a.st;
@@ -622,34 +629,42 @@ __global__ void __launch_bounds__(BLOCK, (W >= 8 ? 2 : (W == 4 ? 3 : 4))) sweep_
     double* coeffs = a.coeffs[cur];
     if (od.kind == OP_GATE || od.kind == OP_PHASE) {
       if (od.kind == OP_GATE && 2 * N > a.cap) {  // uniform: every block reads the same N
-        if (blockIdx.x == 0 && threadIdx.x == 0) st->halt = op;
+        if (grp.bid == 0 && threadIdx.x == 0) st->halt = op;
         break;
       }
       if (threadIdx.x == 0) sgate = reinterpret_cast<const GateDesc<W>*>(a.gates)[od.idx];
       __syncthreads();
       if (od.kind == OP_GATE) {
-        gate_op<W, ALG>(a, sgate, op, N, keys, coeffs, sm);
+        gate_op<W, ALG>(a, sgate, op, N, keys, coeffs, sm, grp);
       } else {
-        phase_op<W, ALG>(sgate, N, keys, coeffs);
-        if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
+        phase_op<W, ALG>(sgate, N, keys, coeffs, grp);
+        if (grp.bid == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
       }
     } else if (od.kind == OP_NOISE_SCALE) {
-      noise_scale_op<W, ALG>(a, a.tables + (u64)od.idx * a.table_len, N, keys, coeffs);
-      if (blockIdx.x == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
+      noise_scale_op<W, ALG>(a, a.tables + (u64)od.idx * a.table_len, N, keys, coeffs, grp);
+      if (grp.bid == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
     } else {
-      for (u64 i = (u64)blockIdx.x * BLOCK + threadIdx.x; i <= a.table_mask; i += (u64)gridDim.x * BLOCK)
+      for (u64 i = (u64)grp.bid * BLOCK + threadIdx.x; i <= a.table_mask; i += (u64)grp.nblk * BLOCK)
         a.table[i] = EMPTY_SLOT;
-      grid_barrier(st, gen);
+      grid_barrier(st, gen, grp);
       noise_compact_op<W, ALG>(a, a.tables + (u64)od.idx * a.table_len, op, N, keys, coeffs, a.keys[cur ^ 1],
-                               a.coeffs[cur ^ 1], sm);
+                               a.coeffs[cur ^ 1], sm, grp);
       cur ^= 1;
     }
-    grid_barrier(st, gen);
+    // In a batch, once enough of the grid sits idle every instance stops at
+    // this op boundary so that the host can hand the idle blocks to the
+    // instances still running.  Block 0 names the op before the barrier and
+    // every block compares it with its own op after it, so all blocks take
+    // the same branch (a block still reading after an earlier barrier sees a
+    // different op and goes on).
+    if (a.idle_blocks && grp.bid == 0 && threadIdx.x == 0 && *(volatile u32*)a.idle_blocks >= a.yield_at)
+      *(volatile u32*)&st->yield_after = op + 1;
+    grid_barrier(st, gen, grp);
     if (*(volatile u32*)&st->error) {
       ++op;
       break;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (grp.bid == 0 && threadIdx.x == 0) {
       const u64 n_new = ld_volatile(&st->n[(op + 1) & 1]);
       a.hist[op] = n_new;
       if (n_new > st->peak) st->peak = n_new;
@@ -659,11 +674,46 @@ __global__ void __launch_bounds__(BLOCK, (W >= 8 ? 2 : (W == 4 ? 3 : 4))) sweep_
         a.stamps[op] = t;
       }
     }
+    if (a.idle_blocks && *(volatile u32*)&st->yield_after == op + 1) {
+      ++op;
+      break;
+    }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (grp.bid == 0 && threadIdx.x == 0) {
     st->cur = (u32)cur;
     st->end_op = op;
+    if (a.idle_blocks) atomicAdd(a.idle_blocks, grp.nblk);
   }
+}
+
+template <int W>
+struct MinBlocks {
+  static constexpr int value = W >= 8 ? 2 : (W == 4 ? 3 : 4);
+};
+
+template <int W, int ALG>
+__global__ void __launch_bounds__(BLOCK, MinBlocks<W>::value) sweep_kernel(const SweepArgs a) {
+  sweep_body<W, ALG>(a, Grp{blockIdx.x, gridDim.x});
+}
+
+// A batch: each instance owns the contiguous blocks [blk_begin, blk_begin +
+// blk_count) of the cooperative grid and runs its own op sequence with its own
+// barrier; block_inst maps a block to its instance.  Instances run at WM or
+// WM / 2 words, so one launch holds, e.g., 64-unit and 128-unit registers.
+template <int WM, int ALG>
+__global__ void __launch_bounds__(BLOCK, MinBlocks<WM>::value) batch_sweep_kernel(const SweepArgs* args,
+                                                                                const u32* block_inst) {
+  __shared__ SweepArgs sa;
+  if (threadIdx.x == 0) sa = args[block_inst[blockIdx.x]];
+  __syncthreads();
+  const Grp grp{blockIdx.x - sa.blk_begin, sa.blk_count};
+  if constexpr (WM > 1) {
+    if (sa.n_words != WM) {
+      sweep_body<WM / 2, ALG>(sa, grp);
+      return;
+    }
+  }
+  sweep_body<WM, ALG>(sa, grp);
 }
 
 // ------------------------------------------------------------ expectation
@@ -833,18 +883,30 @@ __global__ void conjugate_kernel(const u64* keys, const double* coeffs, u64 n, c
 
 }  // namespace
 
+template <class Kernel>
+int co_resident_grid(Kernel k, int blocks_per_sm, int* sms, int* per_sm) {
+  if (!*sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev);
+    int p = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, k, BLOCK, 0);
+    *per_sm = p < 1 ? 1 : p;
+  }
+  const int b = (blocks_per_sm > 0 && blocks_per_sm < *per_sm) ? blocks_per_sm : *per_sm;
+  return *sms * b;
+}
+
 template <int W, int ALG>
 int sweep_grid(int blocks_per_sm) {
   static int sms = 0, per_sm = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<W, ALG>, BLOCK, 0);
-    if (per_sm < 1) per_sm = 1;
-  }
-  const int b = (blocks_per_sm > 0 && blocks_per_sm < per_sm) ? blocks_per_sm : per_sm;
-  return sms * b;
+  return co_resident_grid(sweep_kernel<W, ALG>, blocks_per_sm, &sms, &per_sm);
+}
+
+template <int WM, int ALG>
+int batch_grid(int blocks_per_sm) {
+  static int sms = 0, per_sm = 0;
+  return co_resident_grid(batch_sweep_kernel<WM, ALG>, blocks_per_sm, &sms, &per_sm);
 }
 
 template <int W, int ALG>
@@ -852,6 +914,13 @@ cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s) {
   SweepArgs args = a;
   void* params[] = {&args};
   return cudaLaunchCooperativeKernel((const void*)sweep_kernel<W, ALG>, dim3(grid), dim3(BLOCK), params, 0, s);
+}
+
+template <int W, int ALG>
+cudaError_t launch_batch_sweep(const SweepArgs* args, const u32* block_inst, int grid, cudaStream_t s) {
+  void* params[] = {(void*)&args, (void*)&block_inst};
+  return cudaLaunchCooperativeKernel((const void*)batch_sweep_kernel<W, ALG>, dim3(grid), dim3(BLOCK), params, 0,
+                                     s);
 }
 
 template <int W, int ALG>
@@ -884,7 +953,9 @@ cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const
 
 #define PQ_INSTANTIATE(Wv, Av)                                                                          \
   template int sweep_grid<Wv, Av>(int);                                                                    \
+  template int batch_grid<Wv, Av>(int);                                                                    \
   template cudaError_t launch_sweep<Wv, Av>(const SweepArgs&, int, cudaStream_t);                       \
+  template cudaError_t launch_batch_sweep<Wv, Av>(const SweepArgs*, const u32*, int, cudaStream_t);     \
   template cudaError_t launch_expect<Wv, Av>(const ExpectArgs&, const u64*, const double*, u64,         \
                                              ExpectPartial*, int, cudaStream_t);
 #define PQ_INSTANTIATE_W(Wv)                                                                            \

@@ -34,6 +34,7 @@ struct SweepState {
   u32 error;      // ERR_* bits
   u32 cur;        // row buffer holding the live rows when the sweep ended
   u32 end_op;     // first op the sweep did not run
+  u32 yield_after;  // batched: 1 + the op after which the instance stops early (0 = none)
   u32 bar_count;  // grid barrier: groups arrived
   u32 bar_gen;    // grid barrier generation
   static constexpr unsigned BAR_GROUPS = 16;
@@ -48,6 +49,7 @@ struct SweepArgs {
   const double* tables;    // noise factor tables, table_len entries each
   u32 table_len;
   u32 n_units;
+  u32 n_words;             // W of this propagation's keys
   u32 op_begin, op_end;    // ops [op_begin, op_end) of the sequence
   u32 cur0;                // row buffer holding the live rows at entry
   u32 epoch_base;          // tags this launch's tile statuses
@@ -66,6 +68,9 @@ struct SweepArgs {
   u64* anti;               // anticommuting rows each gate op saw
   u64* stamps;             // %globaltimer at the end of each op
   SweepState* st;
+  u32 blk_begin, blk_count;  // blocks of a batched launch that run this instance
+  u32* idle_blocks;          // batched: blocks whose instance has left the launch (null: never yield)
+  u32 yield_at;              // ... stop at the next op boundary once this many are idle
 };
 
 struct ExpectArgs {
@@ -91,6 +96,14 @@ int sweep_grid(int blocks_per_sm);
 
 template <int W, int ALG>
 cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s);
+// Batched sweep of instances with keys WM or WM / 2 words wide (n_words):
+// args[i] describes instance i and its blk_begin / blk_count slice of the
+// grid; block_inst[b] is the instance of block b.  batch_grid is its
+// co-resident grid, as sweep_grid.
+template <int WM, int ALG>
+int batch_grid(int blocks_per_sm);
+template <int WM, int ALG>
+cudaError_t launch_batch_sweep(const SweepArgs* args, const u32* block_inst, int grid, cudaStream_t s);
 template <int W, int ALG>
 cudaError_t launch_expect(const ExpectArgs& a, const u64* keys, const double* coeffs, u64 n,
                           ExpectPartial* partials, int grid, cudaStream_t s);

@@ -118,7 +118,11 @@ class _Propagator:
     def _make_sum(self, keys, coeffs, observable):
         raise NotImplementedError
 
-    def _run(self, observable, circuit, initial_state, want_terms):
+    def _inputs(self, observable, circuit, initial_state, want_terms):
+        """The engine arguments of one propagation: (RunConfig, obs_words,
+        obs_coeffs, gate_words, angles, layer_offsets, diag_state), the key
+        width and unit count, and the objects the RunConfig points into (they
+        must stay alive until the run returns)."""
         n_units = self._n_units(observable)
         if n_units > MAX_UNITS:
             self._width_error(observable)
@@ -145,8 +149,13 @@ class _Propagator:
         obs_keys, obs_coeffs = observable.to_arrays(n_words)
         gw, ga, off = heisenberg_gates(circuit, n_words, self._key)
         diag = None if initial_state is None else state_words(initial_state, n_units)
+        args = (rc, obs_keys, obs_coeffs, gw, ga, off, diag)
+        return args, n_words, n_units, (tables, plugin, cfg)
+
+    def _run(self, observable, circuit, initial_state, want_terms):
+        args, n_words, n_units, keep = self._inputs(observable, circuit, initial_state, want_terms)
         eng = _native.engine(self.device)
-        res, nt = eng.run(rc, obs_keys, obs_coeffs, gw, ga, off, diag)
+        res, nt = eng.run(*args)
         self.last_run = res
         terms = eng.terms(n_words) if want_terms else None
         if self.logger is not None:
@@ -188,6 +197,40 @@ class _Propagator:
         return observable.n_units()
 
 
+def expectation_values(jobs, blocks_per_sm: int = 0, split: int = 1, rebalance_pct: int = 25, device: int = 0):
+    """Expectation values of many independent propagations in shared
+    persistent launches on one GPU (pq_run_batch).
+
+    `jobs` is a list of (propagator, observable, circuit, initial_state); all
+    propagators are Pauli or all Majorana, each with its own noise and
+    truncation.  Returns one PropagationResult per job, identical to
+    `propagator.expectation_value(observable, circuit, initial_state)`.  The
+    reference runs such sweeps as one call after another
+    (propaq/extrapolators/zne.py:63-108, zce.py:88-137).
+
+    blocks_per_sm: grid size per SM (0 = as many as fit); split: 0 shares the
+    grid equally among the jobs, 1 in proportion to their remaining work;
+    rebalance_pct: re-split the grid among the running jobs once this share of
+    it is idle (0 = never).
+    """
+    jobs = list(jobs)
+    if not jobs:
+        return []
+    items, keep = [], []
+    for prop, observable, circuit, initial_state in jobs:
+        args, _, _, k = prop._inputs(observable, circuit, 0 if initial_state is None else initial_state, False)
+        items.append(args)
+        keep.append(k)
+    eng = _native.engine(device)
+    out = eng.run_batch(items, blocks_per_sm=blocks_per_sm, split=split, rebalance_pct=rebalance_pct)
+    results = []
+    for (prop, *_), (res, nt) in zip(jobs, out):
+        prop.last_run = res
+        results.append(PropagationResult(res.expectation_value, [int(x) for x in nt], res.sparse_key_bytes,
+                                         res.terms_below_cutoff))
+    return results
+
+
 class PauliPropagator(_Propagator):
     """Back-propagates Pauli observables through circuits of Pauli rotations on the GPU."""
 
@@ -225,5 +268,5 @@ class MajoranaPropagator(_Propagator):
         return MajoranaTermSum.from_arrays(keys, coeffs, observable.n_units())
 
 
-__all__ = ["PauliPropagator", "MajoranaPropagator", "PropagationResult", "Logger", "heisenberg_gates",
+__all__ = ["PauliPropagator", "MajoranaPropagator", "PropagationResult", "Logger", "heisenberg_gates", "expectation_values",
            "state_words", "PauliString", "MajoranaMonomial", "words_to_int", "NativeNoiseModel"]

@@ -123,3 +123,38 @@ def majorana_givens(n_sites: int = 32, reps: int = 4, seed: int = 0, max_weight=
         state |= 1 << int(s)
     return Workload(f"majorana_givens_{n_sites}s_r{reps}", 1, n_sites, obs, MajoranaCircuit(layers), max_weight,
                     min_coeff, None, state, meta={"seed": seed, "reps": reps})
+
+
+def most_square_grid(n: int):
+    """(rows, cols) with rows * cols = n and rows the largest divisor <= sqrt(n)."""
+    rows = max(d for d in range(1, math.isqrt(n) + 1) if n % d == 0)
+    return rows, n // rows
+
+
+def kicked_ising_batch(n_instances: int = 64, seed: int = 0, n_range=(40, 100), steps_range=(8, 20),
+                       theta_range=(0.2, 1.0), ps=(0.5e-3, 1e-3, 1.5e-3, 2e-3),
+                       min_coeffs=(1e-3, 1e-4, 1e-5, 1e-6), max_weight=10):
+    """Independent kicked-Ising instances of uneven size, as a zero-noise /
+    zero-cutoff extrapolation sweep runs them: instance i takes noise p and
+    coefficient cutoff from the grid ps x min_coeffs x 4 observable sites
+    (i mod 64), and its qubit count (on the most-square open grid), step count
+    and RX angle from numpy.random.default_rng(seed).  The 4 observables are Z
+    on the centre site and its neighbours up, left and up-left."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_instances):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        theta = float(rng.uniform(*theta_range))
+        g = i % (len(ps) * len(min_coeffs) * 4)
+        p = ps[g // (len(min_coeffs) * 4)]
+        cut = min_coeffs[(g // 4) % len(min_coeffs)]
+        rows, cols = most_square_grid(n)
+        r0, c0 = rows // 2, cols // 2
+        dr, dc = [(0, 0), (-1, 0), (0, -1), (-1, -1)][g % 4]
+        site = max(r0 + dr, 0) * cols + max(c0 + dc, 0)
+        wl = kicked_ising(rows, cols, steps, theta, p, max_weight, cut, site=site)
+        wl.name = f"batch{i}_{rows}x{cols}_s{steps}"
+        wl.meta.update({"index": i, "site": site, "min_coeff": cut})
+        out.append(wl)
+    return out

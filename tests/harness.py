@@ -100,7 +100,8 @@ class GpuResult:
         self.res = res
 
 
-def run_gpu(engine, p: Problem, want_terms=True, noise_plugin=None, truncator=None) -> GpuResult:
+def make_cfg(p: Problem, want_terms=True, noise_plugin=None, truncator=None):
+    """The RunConfig of a problem and the arrays it points into."""
     cfg = _native.RunConfig()
     cfg.basis_kind = p.basis
     cfg.n_units = p.n_units
@@ -121,11 +122,33 @@ def run_gpu(engine, p: Problem, want_terms=True, noise_plugin=None, truncator=No
         cfg.noise_kind, cfg.noise_plugin = _native.PQ_NOISE_PLUGIN, noise_plugin
     cfg.truncator = truncator
     cfg.want_terms = 1 if want_terms else 0
+    return cfg, keep
+
+
+def run_gpu(engine, p: Problem, want_terms=True, noise_plugin=None, truncator=None) -> GpuResult:
+    cfg, keep = make_cfg(p, want_terms, noise_plugin, truncator)
     res, nt = engine.run(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag)
     keys = coeffs = None
     if want_terms:
         keys, coeffs = engine.terms(p.n_words)
     return GpuResult(res, nt, keys, coeffs)
+
+
+def run_gpu_batch(engine, problems, want_terms=True, **tuning) -> list[GpuResult]:
+    """All problems in one pq_run_batch call."""
+    items, keep = [], []
+    for p in problems:
+        cfg, k = make_cfg(p, want_terms)
+        keep.append(k)
+        items.append((cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag))
+    out = engine.run_batch(items, **tuning)
+    results = []
+    for i, (p, (res, nt)) in enumerate(zip(problems, out)):
+        keys = coeffs = None
+        if want_terms:
+            keys, coeffs = engine.terms(p.n_words, index=i)
+        results.append(GpuResult(res, nt, keys, coeffs))
+    return results
 
 
 def sorted_terms(keys: np.ndarray, coeffs: np.ndarray):
