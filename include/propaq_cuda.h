@@ -191,6 +191,28 @@ typedef struct pq_batch_tuning {
  * that instance with pq_run.  tuning NULL = {0, 1, 25}. */
 int pq_run_batch(pq_engine* engine, const pq_instance* instances, size_t n, const pq_batch_tuning* tuning);
 
+/* Expectation value and its gradient with respect to every gate angle,
+ * grad[g] = dE / d gate_angles[g], by reverse-mode differentiation of the
+ * propagation with its truncation decisions (dropped, held and emitted
+ * branches; reclaimed rows) held as the forward run made them.  This entry
+ * point has no counterpart in the reference, whose only derivative-free
+ * parameter sweep is surrogate evaluation (crates/surrogate/src/model.rs:63-107);
+ * it backs a torch.autograd.Function over the propagators.
+ *
+ * Arguments as pq_run; diag_state is required.  The forward run is cut into
+ * segments of checkpoint_layers layers (0 = one segment) whose starting terms
+ * are kept; the reverse pass re-runs one segment at a time while recording
+ * its branches, so device memory grows with one segment's work, not the whole
+ * run's.  Gates deferred into the Clifford frame (fixed Clifford rotations)
+ * get NaN.  A TermBudget floor with a weight cut and a weight-changing
+ * Clifford rotation is refused (PQ_ERR_UNSUPPORTED).  out->device_ms covers
+ * both passes. */
+int pq_run_adjoint(pq_engine* engine, const pq_run_config* cfg, const uint64_t* obs_words,
+                   const double* obs_coeffs, size_t n_obs, const uint64_t* gate_words,
+                   const double* gate_angles, size_t n_gates, const uint32_t* layer_offsets,
+                   size_t n_layers, const uint64_t* diag_state, size_t diag_words,
+                   uint32_t checkpoint_layers, double* grad, uint64_t* n_terms_out, pq_result* out);
+
 /* Final terms of instance `index` of the last batch (index 0 after pq_run),
  * as pq_result_terms. */
 size_t pq_result_terms_at(pq_engine* engine, size_t index, uint64_t* keys, double* coeffs, size_t cap);

@@ -121,6 +121,8 @@ _SIGNATURES = {
     "pq_result_terms": (_Z, [_V, _V, _V, _Z]),
     "pq_run_batch": (ctypes.c_int, [_V, ctypes.POINTER(Instance), _Z, ctypes.POINTER(BatchTuning)]),
     "pq_result_terms_at": (_Z, [_V, _Z, _V, _V, _Z]),
+    "pq_run_adjoint": (ctypes.c_int, [_V, ctypes.POINTER(RunConfig), _V, _V, _Z, _V, _V, _Z, _V, _Z, _V, _Z, _U32,
+                                      _V, _V, ctypes.POINTER(RunResult)]),
     "pq_plugin_load_noise": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_V),
                                             ctypes.c_char_p, _Z]),
     "pq_plugin_load_truncator": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_V),
@@ -204,6 +206,28 @@ class Engine:
             if rc != PQ_OK:
                 raise_for(rc, lib().pq_engine_last_error(self._h).decode(errors="replace"))
         return res, nt
+
+    def run_adjoint(self, cfg: RunConfig, obs_words, obs_coeffs, gate_words, gate_angles, layer_offsets,
+                    diag_state, checkpoint_layers: int = 0):
+        """Runs pq_run_adjoint; returns (RunResult, n_terms array, dE/d gate_angles)."""
+        obs_words = np.ascontiguousarray(obs_words, dtype=np.uint64)
+        obs_coeffs = np.ascontiguousarray(obs_coeffs, dtype=np.float64)
+        gate_words = np.ascontiguousarray(gate_words, dtype=np.uint64)
+        gate_angles = np.ascontiguousarray(gate_angles, dtype=np.float64)
+        layer_offsets = np.ascontiguousarray(layer_offsets, dtype=np.uint32)
+        diag = np.ascontiguousarray(diag_state, dtype=np.uint64)
+        n_gates = len(gate_angles)
+        nt = np.zeros(n_gates, dtype=np.uint64)
+        grad = np.zeros(n_gates, dtype=np.float64)
+        res = RunResult()
+        with self.lock:
+            rc = lib().pq_run_adjoint(self._h, ctypes.byref(cfg), _ptr(obs_words), _ptr(obs_coeffs), len(obs_coeffs),
+                                      _ptr(gate_words), _ptr(gate_angles), n_gates, _ptr(layer_offsets),
+                                      len(layer_offsets) - 1, _ptr(diag), len(diag), checkpoint_layers, _ptr(grad),
+                                      _ptr(nt), ctypes.byref(res))
+            if rc != PQ_OK:
+                raise_for(rc, lib().pq_engine_last_error(self._h).decode(errors="replace"))
+        return res, nt, grad
 
     def run_batch(self, items, blocks_per_sm: int = 0, split: int = 1, rebalance_pct: int = 25,
                   want_n_terms: bool = True):

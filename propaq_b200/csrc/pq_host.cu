@@ -610,6 +610,8 @@ struct Plan {
   std::vector<u64> gdesc;  // GateDesc<W> records back to back
   size_t n_gdesc = 0;
   std::vector<long> gate_op;  // latest op at or before each gate, -1 = none
+  std::vector<char> gate_own;  // the gate has an op of its own (not deferred into the frame)
+  std::vector<size_t> layer_op;  // first op of each layer
   Tableau frame{0, 1, 0};
   long last_op = -1;
   size_t done = 0, uploaded_ops = 0, uploaded_gdesc = 0;
@@ -703,6 +705,7 @@ int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
   P.n_live = P.peak = P.n0;
   P.frame = Tableau(ALG, W, P.n_units);
   P.gate_op.assign(in.n_gates, -1);
+  P.gate_own.assign(in.n_gates, 0);
   P.ops.reserve(in.n_gates + in.n_layers);
   P.gdesc.reserve(in.n_gates * gdesc_words(W));
   return PQ_OK;
@@ -760,6 +763,7 @@ int build_ops(Plan& P, NeedN need_n) {
   const int W = P.W, ALG = P.alg;
   std::vector<u64> g(W), gc(W);
   for (size_t l = 0; l < in.n_layers; ++l) {
+    P.layer_op.push_back(P.ops.size());
     if (P.have_noise) {
       pq::OpDesc od;
       od.kind = (P.has_w || P.has_c) ? pq::OP_NOISE_COMPACT : pq::OP_NOISE_SCALE;  // partitioned_termsum.rs:585-587
@@ -803,8 +807,10 @@ int build_ops(Plan& P, NeedN need_n) {
       P.ops.push_back(od);
       P.last_op = (long)P.ops.size() - 1;
       P.gate_op[gi] = P.last_op;
+      P.gate_own[gi] = 1;
     }
   }
+  P.layer_op.push_back(P.ops.size());
   return PQ_OK;
 }
 
@@ -822,7 +828,17 @@ void upload_ops(pq_engine* E, Slot& S, Plan& P) {
   }
 }
 
-pq::SweepArgs sweep_args(Slot& S, const Plan& P, pq::SweepState* st, u32 blk_begin, u32 blk_count) {
+// Device arrays of the adjoint's recording (see SweepArgs::rec_idx).
+struct Recording {
+  u32* idx = nullptr;
+  double* coef = nullptr;
+  u64* keys = nullptr;
+  u64* off = nullptr;
+  u64* key_off = nullptr;
+};
+
+pq::SweepArgs sweep_args(Slot& S, const Plan& P, pq::SweepState* st, u32 blk_begin, u32 blk_count,
+                         size_t op_limit = (size_t)-1, const Recording* rec = nullptr) {
   pq::SweepArgs a{};
   a.ops = S.d_ops;
   a.gates = S.d_gates;
@@ -831,7 +847,14 @@ pq::SweepArgs sweep_args(Slot& S, const Plan& P, pq::SweepState* st, u32 blk_beg
   a.n_units = P.n_units;
   a.n_words = (u32)P.W;
   a.op_begin = (u32)P.done;
-  a.op_end = (u32)P.ops.size();
+  a.op_end = (u32)std::min(op_limit, P.ops.size());
+  if (rec) {
+    a.rec_idx = rec->idx;
+    a.rec_coef = rec->coef;
+    a.rec_keys = rec->keys;
+    a.rec_off = rec->off;
+    a.rec_key_off = rec->key_off;
+  }
   a.cur0 = (u32)S.cur;
   a.epoch_base = S.epoch_base;
   a.max_weight = P.wcut;
@@ -893,14 +916,16 @@ int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
 
 // Runs every built op of one plan on the whole grid, relaunching after
 // capacity growth.
-int execute_single(pq_engine* E, Slot& S, Plan& P, int grid, bool* began) {
+int execute_single(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size_t op_limit = (size_t)-1,
+                   const Recording* rec = nullptr) {
   cudaError_t e;
   upload_ops(E, S, P);
-  while (P.done < P.ops.size()) {
+  const size_t end = std::min(op_limit, P.ops.size());
+  while (P.done < end) {
     E->h_states[0] = fresh_state(P);
     cudaMemcpyAsync(E->d_states, E->h_states, sizeof(pq::SweepState), cudaMemcpyHostToDevice, E->stream);
-    cudaMemsetAsync(S.tickets + P.done, 0, (P.ops.size() - P.done) * 4, E->stream);
-    const pq::SweepArgs a = sweep_args(S, P, E->d_states, 0, (u32)grid);
+    cudaMemsetAsync(S.tickets + P.done, 0, (end - P.done) * 4, E->stream);
+    const pq::SweepArgs a = sweep_args(S, P, E->d_states, 0, (u32)grid, end, rec);
     if (!*began) {  // device time starts at the first sweep
       cudaEventRecord(E->ev_begin, E->stream);
       *began = true;
@@ -921,6 +946,28 @@ int execute_single(pq_engine* E, Slot& S, Plan& P, int grid, bool* began) {
     if (int rc = absorb_state(E, S, P, E->h_states[0])) return rc;
   }
   return PQ_OK;
+}
+
+// Arguments of the readout kernels: the basis state in key layout and the
+// frame (uploaded by finalize).
+pq::ExpectArgs expect_args(const Slot& S, const Plan& P) {
+  const Inputs& in = *P.in;
+  pq::ExpectArgs xa{};
+  if (in.diag) {
+    for (u32 u = 0; u < P.n_units; ++u) {
+      const u64 bit = (u / 64 < in.nd) ? (in.diag[u / 64] >> (u % 64)) & 1 : 0;
+      if (!bit) continue;
+      const u32 pos = P.alg == 0 ? 2 * u + 1 : 2 * u;
+      if (pos / 64 < (u32)P.W) xa.state[pos / 64] |= 1ULL << (pos % 64);
+    }
+  }
+  xa.n_units = P.n_units;
+  xa.has_min_coeff = P.has_c;
+  xa.min_coeff = P.ccut;
+  xa.frame_images = P.frame.identity ? nullptr : S.frame_img;
+  xa.frame_signs = P.frame.identity ? nullptr : S.frame_sgn;
+  xa.frame_rows = (u32)P.frame.rows;
+  return xa;
 }
 
 // Enqueues the expectation value and the final-term readout of one plan.
@@ -948,21 +995,7 @@ int finalize(pq_engine* E, Slot& S, Plan& P, std::vector<pq::ExpectPartial>* par
   const int* d_sgn = P.frame.identity ? nullptr : S.frame_sgn;
   parts->clear();
   if (in.diag || P.has_c) {
-    pq::ExpectArgs xa{};
-    if (in.diag) {
-      for (u32 u = 0; u < P.n_units; ++u) {
-        const u64 bit = (u / 64 < in.nd) ? (in.diag[u / 64] >> (u % 64)) & 1 : 0;
-        if (!bit) continue;
-        const u32 pos = ALG == 0 ? 2 * u + 1 : 2 * u;
-        if (pos / 64 < (u32)W) xa.state[pos / 64] |= 1ULL << (pos % 64);
-      }
-    }
-    xa.n_units = P.n_units;
-    xa.has_min_coeff = P.has_c;
-    xa.min_coeff = P.ccut;
-    xa.frame_images = d_img;
-    xa.frame_signs = d_sgn;
-    xa.frame_rows = (u32)P.frame.rows;
+    const pq::ExpectArgs xa = expect_args(S, P);
     ++E->launches;
     e = with_words(W, [&](auto w) {
       constexpr int WW = decltype(w)::value;
@@ -1096,6 +1129,206 @@ int run_one(pq_engine* E, const Inputs& in, int W) {
   cudaEventRecord(E->ev_end, E->stream);
   if (cudaError_t e = cudaStreamSynchronize(E->stream)) return E->cuda_fail(e, "finalize");
   if (int rc = finish(E, S, P, parts)) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, E->ev_begin, E->ev_end);
+  in.res->device_ms = ms;
+  return PQ_OK;
+}
+
+// Device buffers of one adjoint run, freed on every exit path.
+struct RunBuffers {
+  std::vector<void*> ptrs;
+  ~RunBuffers() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  cudaError_t alloc(T** p, size_t n) {
+    *p = nullptr;
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T));
+    if (e == cudaSuccess) ptrs.push_back(*p);
+    return e;
+  }
+};
+
+// Expectation value and dE/d(angle) of every gate with the truncation
+// decisions of the forward run held fixed.  The forward run is split into
+// segments of ckpt_layers layers and keeps the live terms at the start of
+// each.  Then, last segment first, it restores a segment's start, runs the
+// segment again while recording each op's sin branches and reclaim maps
+// (SweepArgs::rec_idx), and runs the reverse sweep over it (adjoint_kernel),
+// which carries dE/dc back to the segment's start.  Device memory: the
+// checkpoints, plus 12 bytes per row entering each op of one segment (and
+// 8W + 4 per row entering each reclaim).
+int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, double* grad_out) {
+  if (!in.diag) return E->fail(PQ_ERR_INVALID, "the gradient needs an initial state");
+  if (int rc = E->ensure_slots(1)) return rc;
+  Slot& S = E->slots[0];
+  Plan P;
+  if (int rc = prepare(E, P, in, W)) return rc;
+  if (int rc = setup_slot(E, S, P)) return rc;
+  const int ALG = P.alg;
+  const int grid = with_words(W, [&](auto w) {
+    constexpr int WW = decltype(w)::value;
+    return ALG == 0 ? pq::sweep_grid<WW, 0>((int)in.cfg->blocks_per_sm)
+                    : pq::sweep_grid<WW, 1>((int)in.cfg->blocks_per_sm);
+  });
+  const int agrid = with_words(W, [&](auto w) {
+    constexpr int WW = decltype(w)::value;
+    return ALG == 0 ? pq::adjoint_grid<WW, 0>() : pq::adjoint_grid<WW, 1>();
+  });
+  auto no_sync = [&](u64*) -> int {
+    return E->fail(PQ_ERR_UNSUPPORTED,
+                   "the gradient cannot decide Clifford deferral under a TermBudget floor with a weight cut");
+  };
+  if (int rc = build_ops(P, no_sync)) return rc;
+  const size_t n_ops = P.ops.size();
+  const size_t per = ckpt_layers ? ckpt_layers : std::max<size_t>(in.n_layers, 1);
+  std::vector<size_t> seg;
+  for (size_t l = 0; l < in.n_layers; l += per) seg.push_back(P.layer_op[l]);
+  seg.push_back(n_ops);
+  const size_t n_seg = seg.size() - 1;
+  RunBuffers mem;
+  cudaError_t e;
+
+  // Forward, keeping each segment's starting terms.
+  std::vector<u64*> ck_keys(n_seg, nullptr);
+  std::vector<double*> ck_coeffs(n_seg, nullptr);
+  std::vector<u64> ck_n(n_seg, 0);
+  bool began = false;
+  for (size_t s = 0; s < n_seg; ++s) {
+    ck_n[s] = P.n_live;
+    if ((e = mem.alloc(&ck_keys[s], ck_n[s] * W)) != cudaSuccess ||
+        (e = mem.alloc(&ck_coeffs[s], ck_n[s])) != cudaSuccess)
+      return E->cuda_fail(e, "checkpoint");
+    cudaMemcpyAsync(ck_keys[s], S.keys[S.cur], ck_n[s] * W * 8, cudaMemcpyDeviceToDevice, E->stream);
+    cudaMemcpyAsync(ck_coeffs[s], S.coeffs[S.cur], ck_n[s] * 8, cudaMemcpyDeviceToDevice, E->stream);
+    if (int rc = execute_single(E, S, P, grid, &began, seg[s + 1])) return rc;
+  }
+  if (!began) cudaEventRecord(E->ev_begin, E->stream);
+  std::vector<pq::ExpectPartial> parts;
+  if (int rc = finalize(E, S, P, &parts)) return rc;
+  if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "expectation");
+  if (int rc = finish(E, S, P, parts)) return rc;
+  const u64 n_fin = P.n_live;
+
+  // Rows entering each op, recording offsets, gate -> op map.
+  std::vector<u64> hist(n_ops), n_in(n_ops), off(n_ops, 0), koff(n_ops, 0);
+  if (n_ops) cudaMemcpy(hist.data(), S.hist, n_ops * 8, cudaMemcpyDeviceToHost);
+  for (size_t k = 0; k < n_ops; ++k) n_in[k] = k ? hist[k - 1] : P.n0;
+  size_t max_rec = 0, max_krec = 0;
+  for (size_t s = 0; s < n_seg; ++s) {
+    size_t tot = 0, ktot = 0;
+    for (size_t k = seg[s]; k < seg[s + 1]; ++k) {
+      if (P.ops[k].kind != pq::OP_NOISE_SCALE) {
+        off[k] = tot;
+        tot += n_in[k];
+      }
+      if (P.ops[k].kind == pq::OP_NOISE_COMPACT) {
+        koff[k] = ktot;
+        ktot += n_in[k];
+      }
+    }
+    max_rec = std::max(max_rec, tot);
+    max_krec = std::max(max_krec, ktot);
+  }
+  std::vector<long long> gate_ops(in.n_gates);
+  for (size_t g = 0; g < in.n_gates; ++g) gate_ops[g] = P.gate_own[g] ? P.gate_op[g] : -1;
+  Recording rec;
+  double* lam[2] = {nullptr, nullptr};
+  double* grad_part = nullptr;
+  double* d_grad = nullptr;
+  u64* d_n_in = nullptr;
+  long long* d_gate_ops = nullptr;
+  const u64** d_ksrc = nullptr;
+  if ((e = mem.alloc(&rec.idx, max_rec)) != cudaSuccess || (e = mem.alloc(&rec.coef, max_rec)) != cudaSuccess ||
+      (e = mem.alloc(&rec.keys, max_krec * W)) != cudaSuccess || (e = mem.alloc(&rec.off, n_ops)) != cudaSuccess ||
+      (e = mem.alloc(&rec.key_off, n_ops)) != cudaSuccess || (e = mem.alloc(&lam[0], S.cap)) != cudaSuccess ||
+      (e = mem.alloc(&lam[1], S.cap)) != cudaSuccess ||
+      (e = mem.alloc(&grad_part, n_ops * (size_t)agrid)) != cudaSuccess ||
+      (e = mem.alloc(&d_grad, in.n_gates)) != cudaSuccess || (e = mem.alloc(&d_n_in, n_ops)) != cudaSuccess ||
+      (e = mem.alloc(&d_gate_ops, in.n_gates)) != cudaSuccess || (e = mem.alloc(&d_ksrc, n_ops)) != cudaSuccess)
+    return E->cuda_fail(e, "adjoint buffers");
+  if (n_ops) {
+    cudaMemcpyAsync(rec.off, off.data(), n_ops * 8, cudaMemcpyHostToDevice, E->stream);
+    cudaMemcpyAsync(rec.key_off, koff.data(), n_ops * 8, cudaMemcpyHostToDevice, E->stream);
+    cudaMemcpyAsync(d_n_in, n_in.data(), n_ops * 8, cudaMemcpyHostToDevice, E->stream);
+    cudaMemsetAsync(grad_part, 0, n_ops * (size_t)agrid * 8, E->stream);
+  }
+  if (in.n_gates)
+    cudaMemcpyAsync(d_gate_ops, gate_ops.data(), in.n_gates * 8, cudaMemcpyHostToDevice, E->stream);
+
+  // Seed: dE/dc of the final rows.
+  const pq::ExpectArgs xa = expect_args(S, P);
+  ++E->launches;
+  e = with_words(W, [&](auto w) {
+    constexpr int WW = decltype(w)::value;
+    return ALG == 0 ? pq::launch_adjoint_seed<WW, 0>(xa, S.keys[S.cur], n_fin, lam[0], E->stream)
+                    : pq::launch_adjoint_seed<WW, 1>(xa, S.keys[S.cur], n_fin, lam[0], E->stream);
+  });
+  if (e != cudaSuccess) return E->cuda_fail(e, "adjoint seed");
+  int lam_cur = 0;
+
+  // Reverse, one segment at a time.
+  for (size_t s = n_seg; s-- > 0;) {
+    if (seg[s] == seg[s + 1]) continue;
+    if (ck_n[s]) {
+      cudaMemcpyAsync(S.keys[0], ck_keys[s], ck_n[s] * W * 8, cudaMemcpyDeviceToDevice, E->stream);
+      cudaMemcpyAsync(S.coeffs[0], ck_coeffs[s], ck_n[s] * 8, cudaMemcpyDeviceToDevice, E->stream);
+    }
+    S.cur = 0;
+    if (int rc = E->rebuild_table(S, ck_n[s])) return rc;
+    P.done = seg[s];
+    P.n_live = ck_n[s];
+    if (int rc = execute_single(E, S, P, grid, &began, seg[s + 1], &rec)) return rc;
+    // Keys of each op's input rows: the snapshot of the next reclaim of the
+    // segment (rows only grow until then), else the segment's last buffer.
+    std::vector<const u64*> ksrc(seg[s + 1] - seg[s]);
+    const u64* next = S.keys[S.cur];
+    for (size_t k = seg[s + 1]; k-- > seg[s];) {
+      if (P.ops[k].kind == pq::OP_NOISE_COMPACT) next = rec.keys + koff[k] * W;
+      ksrc[k - seg[s]] = next;
+    }
+    cudaMemcpyAsync(d_ksrc + seg[s], ksrc.data(), ksrc.size() * sizeof(u64*), cudaMemcpyHostToDevice, E->stream);
+    E->h_states[0] = pq::SweepState{};
+    cudaMemcpyAsync(E->d_states, E->h_states, sizeof(pq::SweepState), cudaMemcpyHostToDevice, E->stream);
+    pq::AdjointArgs aa{};
+    aa.ops = S.d_ops;
+    aa.gates = S.d_gates;
+    aa.tables = S.d_tables;
+    aa.table_len = (u32)P.tlen;
+    aa.n_units = P.n_units;
+    aa.op_begin = (u32)seg[s];
+    aa.op_end = (u32)seg[s + 1];
+    aa.cur0 = (u32)lam_cur;
+    aa.n_in = d_n_in;
+    aa.rec_idx = rec.idx;
+    aa.rec_coef = rec.coef;
+    aa.rec_off = rec.off;
+    aa.key_src = d_ksrc;
+    aa.lam[0] = lam[0];
+    aa.lam[1] = lam[1];
+    aa.grad_part = grad_part;
+    aa.st = E->d_states;
+    ++E->launches;
+    e = with_words(W, [&](auto w) {
+      constexpr int WW = decltype(w)::value;
+      return ALG == 0 ? pq::launch_adjoint<WW, 0>(aa, agrid, E->stream) : pq::launch_adjoint<WW, 1>(aa, agrid, E->stream);
+    });
+    if (e != cudaSuccess) return E->cuda_fail(e, "adjoint launch");
+    cudaMemcpyAsync(E->h_states, E->d_states, sizeof(pq::SweepState), cudaMemcpyDeviceToHost, E->stream);
+    if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "adjoint");
+    if (E->h_states[0].error & pq::ERR_BARRIER_TIMEOUT)
+      return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a grid barrier wait expired on the device");
+    if (E->h_states[0].error) return E->fail(PQ_ERR_CUDA, "device reported error bits " +
+                                                             std::to_string(E->h_states[0].error));
+    lam_cur = (int)E->h_states[0].cur;
+  }
+  ++E->launches;
+  if ((e = pq::launch_grad_reduce(grad_part, agrid, d_gate_ops, in.n_gates, d_grad, E->stream)) != cudaSuccess)
+    return E->cuda_fail(e, "gradient reduction");
+  if (in.n_gates) cudaMemcpyAsync(grad_out, d_grad, in.n_gates * 8, cudaMemcpyDeviceToHost, E->stream);
+  cudaEventRecord(E->ev_end, E->stream);
+  if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "gradient");
   float ms = 0;
   cudaEventElapsedTime(&ms, E->ev_begin, E->ev_end);
   in.res->device_ms = ms;
@@ -1336,6 +1569,22 @@ int pq_run_batch(pq_engine* E, const pq_instance* insts, size_t n, const pq_batc
   const u64 l0 = E->launches;
   const int rc = run_batch(E, ins, WM, tune);
   for (size_t i = 0; i < n; ++i) insts[i].result->gpu_launches = E->launches - l0;
+  return rc;
+}
+
+int pq_run_adjoint(pq_engine* E, const pq_run_config* cfg, const uint64_t* ow, const double* oc, size_t no,
+                   const uint64_t* gw, const double* ga, size_t ng, const uint32_t* lo, size_t nl, const uint64_t* d,
+                   size_t nd, uint32_t checkpoint_layers, double* grad, uint64_t* nt, pq_result* r) {
+  if (!E || !cfg || !r || (ng && !grad)) return PQ_ERR_INVALID;
+  std::memset(r, 0, sizeof(*r));
+  E->err.clear();
+  int W = 0;
+  if (int rc = check_inputs(E, cfg, ng, lo, nl, &W)) return rc;
+  if (cudaSetDevice(E->device) != cudaSuccess) return E->fail(PQ_ERR_CUDA, "cudaSetDevice failed");
+  const u64 l0 = E->launches;
+  const Inputs in{cfg, K(ow), oc, no, K(gw), ga, ng, lo, nl, K(d), nd, reinterpret_cast<u64*>(nt), r, W};
+  const int rc = run_adjoint(E, in, W, checkpoint_layers, grad);
+  r->gpu_launches = E->launches - l0;
   return rc;
 }
 

@@ -298,6 +298,23 @@ __device__ __forceinline__ void tile_scan(u32 flags, unsigned* masks, TileSmem& 
   __syncthreads();
 }
 
+// Adjoint recording of one gate's sin branches (see SweepArgs::rec_idx).  A
+// source without a partner row records REC_NONE here; its child's row
+// replaces it once the child is placed.
+__device__ __forceinline__ void record_single(const SweepArgs& a, u32 op, u64 r, double c) {
+  const u64 o = a.rec_off[op];
+  a.rec_coef[o + r] = c;
+  a.rec_idx[o + r] = REC_NONE;
+}
+__device__ __forceinline__ void record_pair(const SweepArgs& a, u32 op, u64 r, u64 j, double c, double cj, bool to_j,
+                                            bool to_i) {
+  const u64 o = a.rec_off[op];
+  a.rec_coef[o + r] = c;
+  a.rec_coef[o + j] = cj;
+  a.rec_idx[o + r] = to_j ? (u32)j : REC_NONE;
+  a.rec_idx[o + j] = to_i ? (u32)r : REC_NONE;
+}
+
 // ------------------------------------------------------------------ gate
 // Tiles are assigned statically (tile t to block t mod grid, in order); the
 // cooperative launch keeps every block resident, so a tile's look-back always
@@ -380,6 +397,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
           emit |= 1u << k;
           bval[k] = bi;
         }
+        if (a.rec_idx) record_single(a, op, r, c[k]);
       } else {
         const double bj = __dmul_rn(__dmul_rn(cj[k], sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
         const int sj = state(cj[k], key[k]);
@@ -391,6 +409,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
         if (to_j) nj = __dadd_rn(nj, bi);
         coeffs[r] = ni;
         coeffs[j[k]] = nj;
+        if (a.rec_idx) record_pair(a, op, r, (u64)j[k], c[k], cj[k], to_j, to_i);
       }
     }
     unsigned masks[IT];
@@ -410,6 +429,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
       store_key<W>(keys, row, q);
       coeffs[row] = bval[k];
       insert<W>(q, row, a.table, a.table_mask, &st->error);
+      if (a.rec_idx) a.rec_idx[a.rec_off[op] + (u64)t * TL + (u64)k * BLOCK + threadIdx.x] = (u32)row;
     }
     __syncthreads();  // sm is reused by the next tile
   }
@@ -473,6 +493,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
           emit |= 1u << k;
           bval[k] = bi;
         }
+        if (a.rec_idx) record_single(a, op, r, c);
       } else {
         const double cj = __ldcg(coeffs + j);
         const double bj = __dmul_rn(__dmul_rn(cj, sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
@@ -485,6 +506,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
         if (to_j) nj = __dadd_rn(nj, bi);
         coeffs[r] = ni;
         coeffs[j] = nj;
+        if (a.rec_idx) record_pair(a, op, r, (u64)j, c, cj, to_j, to_i);
       }
     }
     unsigned masks[IT];
@@ -506,6 +528,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
       store_key<W>(keys, row, q);
       coeffs[row] = bval[k];
       insert<W>(q, row, a.table, a.table_mask, &st->error);
+      if (a.rec_idx) a.rec_idx[a.rec_off[op] + r] = (u32)row;
     }
     __syncthreads();
   }
@@ -532,12 +555,17 @@ __device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d
 // A rotation with |sin| < 1e-9 only scales the anticommuting rows by cos
 // (partitioned_termsum.rs:303-308, termsum.rs:551-557).
 template <int W, int ALG>
-__device__ __noinline__ void phase_op(const GateDesc<W>& d, u64 N, const u64* keys, double* coeffs, const Grp grp) {
+__device__ __noinline__ void phase_op(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, const u64* keys,
+                                      double* coeffs, const Grp grp) {
   using Ops = typename Alg<ALG>::T;
   for (u64 r = (u64)grp.bid * BLOCK + threadIdx.x; r < N; r += (u64)grp.nblk * BLOCK) {
     u64 key[W];
     load_key<W>(keys, r, key);
-    if (Ops::template anticommutes<W>(d.g, key)) coeffs[r] = __dmul_rn(__ldcg(coeffs + r), d.cs);
+    if (Ops::template anticommutes<W>(d.g, key)) {
+      const double c = __ldcg(coeffs + r);
+      coeffs[r] = __dmul_rn(c, d.cs);
+      if (a.rec_idx) a.rec_coef[a.rec_off[op] + r] = c;
+    }
   }
 }
 
@@ -597,6 +625,10 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
       const bool kp = (a.max_weight == NO_WEIGHT_CUT || w <= a.max_weight) &&
                       (!a.has_min_coeff || fabs(c) >= a.min_coeff);
       keep |= (u32)kp << k;
+      if (a.rec_idx) {
+        a.rec_idx[a.rec_off[op] + r] = REC_NONE;
+        store_key<W>(a.rec_keys + a.rec_key_off[op] * W, r, key[k]);
+      }
     }
     unsigned masks[IT];
     tile_scan<IT>(keep, masks, sm, a.status, t, ntiles, 0, epoch, st, n_out);
@@ -608,6 +640,7 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
       store_key<W>(keys_out, row, key[k]);
       coeffs_out[row] = cv[k];
       insert<W>(key[k], row, a.table, a.table_mask, &st->error);
+      if (a.rec_idx) a.rec_idx[a.rec_off[op] + (u64)t * TL + (u64)k * BLOCK + threadIdx.x] = (u32)row;
     }
     __syncthreads();
   }
@@ -637,7 +670,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
       if (od.kind == OP_GATE) {
         gate_op<W, ALG>(a, sgate, op, N, keys, coeffs, sm, grp);
       } else {
-        phase_op<W, ALG>(sgate, N, keys, coeffs, grp);
+        phase_op<W, ALG>(a, sgate, op, N, keys, coeffs, grp);
         if (grp.bid == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
       }
     } else if (od.kind == OP_NOISE_SCALE) {
@@ -860,6 +893,140 @@ __global__ void __launch_bounds__(BLOCK) expect_kernel(const ExpectArgs a, const
   }
 }
 
+// ------------------------------------------------------------ adjoint
+// Reverse sweep of one recorded segment.  With the truncation decisions of the
+// forward run frozen, each op is linear in the coefficients, so dE/dc of its
+// input rows is the transpose of the op applied to dE/dc of its output rows:
+//   gate, row r anticommuting with G, coefficient c, sin branch to row p:
+//     lam_in[r] = cos * lam_out[r] + sin * s_r * lam_out[p]
+//     dE/dangle += -sin * c * lam_out[r] + cos * s_r * c * lam_out[p]
+//   (s_r = -Im of the phase of G K_r, times the frame sign of G), and
+//   lam_in[r] = lam_out[r] for commuting rows;
+//   noise: lam_in[r] = f(w_r) * lam_out[new index of r] (0 if dropped).
+// lam_out was written by other blocks during the previous op, so it is read
+// through L2 (ld.cg).
+
+__device__ __forceinline__ void block_partial(double v, double* out) {
+  __shared__ double red[NWARPS];
+  for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_xor_sync(FULL, v, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < NWARPS; ++w) t = __dadd_rn(t, red[w]);
+    *out = t;
+  }
+  __syncthreads();
+}
+
+template <int W, int ALG>
+__device__ __noinline__ void adjoint_gate(const AdjointArgs& a, const GateDesc<W>& d, u32 op, bool phase, u64 N,
+                                          const u64* keys, const double* lin, double* lout) {
+  using Ops = typename Alg<ALG>::T;
+  const u64 o = a.rec_off[op];
+  double gsum = 0.0;
+  for (u64 r = (u64)blockIdx.x * BLOCK + threadIdx.x; r < N; r += (u64)gridDim.x * BLOCK) {
+    u64 key[W];
+    load_key<W>(keys, r, key);
+    const double l = __ldcg(lin + r);
+    if (!Ops::template anticommutes<W>(d.g, key)) {
+      lout[r] = l;
+      continue;
+    }
+    const double c = __ldg(a.rec_coef + o + r);
+    double v = __dmul_rn(d.cs, l);
+    gsum = __dadd_rn(gsum, -__dmul_rn(__dmul_rn(d.sn, c), l));
+    const u32 p = phase ? REC_NONE : __ldg(a.rec_idx + o + r);
+    if (p != REC_NONE) {
+      const double sr = neg_im(Ops::template product_exp<W>(d.g, key), d.g.sign);
+      const double lp = __ldcg(lin + p);
+      v = __dadd_rn(v, __dmul_rn(__dmul_rn(d.sn, sr), lp));
+      gsum = __dadd_rn(gsum, __dmul_rn(__dmul_rn(__dmul_rn(d.cs, sr), c), lp));
+    }
+    lout[r] = v;
+  }
+  block_partial(gsum, a.grad_part + (u64)op * gridDim.x + blockIdx.x);
+}
+
+template <int W, int ALG>
+__device__ __noinline__ void adjoint_noise(const AdjointArgs& a, const double* factors, u32 op, bool compact, u64 N,
+                                           const u64* keys, const double* lin, double* lout) {
+  using Ops = typename Alg<ALG>::T;
+  const u32 last = a.table_len - 1;
+  const u64 o = a.rec_off[op];
+  for (u64 r = (u64)blockIdx.x * BLOCK + threadIdx.x; r < N; r += (u64)gridDim.x * BLOCK) {
+    u64 key[W];
+    load_key<W>(keys, r, key);
+    const u32 w = Ops::template weight<W>(key, a.n_units);
+    const double f = __ldg(factors + (w < last ? w : last));
+    if (compact) {
+      const u32 p = __ldg(a.rec_idx + o + r);
+      lout[r] = p == REC_NONE ? 0.0 : __dmul_rn(f, __ldcg(lin + p));
+    } else {
+      lout[r] = __dmul_rn(f, __ldcg(lin + r));
+    }
+  }
+}
+
+template <int W, int ALG>
+__global__ void __launch_bounds__(BLOCK, MinBlocks<W>::value) adjoint_kernel(const AdjointArgs a) {
+  __shared__ GateDesc<W> sgate;
+  const Grp grp{blockIdx.x, gridDim.x};
+  SweepState* st = a.st;
+  u32 gen = *(volatile u32*)&st->bar_gen;
+  int cur = (int)a.cur0;
+  for (u32 op = a.op_end; op-- > a.op_begin;) {
+    const OpDesc od = a.ops[op];
+    const u64 N = a.n_in[op];
+    const u64* keys = a.key_src[op];
+    const double* lin = a.lam[cur];
+    double* lout = a.lam[cur ^ 1];
+    if (od.kind == OP_GATE || od.kind == OP_PHASE) {
+      if (threadIdx.x == 0) sgate = reinterpret_cast<const GateDesc<W>*>(a.gates)[od.idx];
+      __syncthreads();
+      adjoint_gate<W, ALG>(a, sgate, op, od.kind == OP_PHASE, N, keys, lin, lout);
+    } else {
+      adjoint_noise<W, ALG>(a, a.tables + (u64)od.idx * a.table_len, op, od.kind == OP_NOISE_COMPACT, N, keys, lin,
+                            lout);
+    }
+    cur ^= 1;
+    grid_barrier(st, gen, grp);
+    if (*(volatile u32*)&st->error) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->cur = (u32)cur;
+}
+
+template <int W, int ALG>
+__global__ void adjoint_seed_kernel(const ExpectArgs a, const u64* keys, u64 N, double* lam) {
+  using Ops = typename Alg<ALG>::T;
+  for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (u64)gridDim.x * blockDim.x) {
+    u64 key[W];
+    load_key<W>(keys, r, key);
+    if (a.frame_images) {
+      u64 img[W];
+      const double sg = conjugate_key<W, ALG>(key, a.frame_images, a.frame_signs, a.frame_rows, img);
+      lam[r] = __dmul_rn(sg, Ops::template trace<W>(img, a.state, a.n_units));
+    } else {
+      lam[r] = Ops::template trace<W>(key, a.state, a.n_units);
+    }
+  }
+}
+
+__global__ void grad_reduce_kernel(const double* grad_part, int grid, const long long* gate_ops, u64 n_gates,
+                                   double* grad) {
+  for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < n_gates; g += (u64)gridDim.x * blockDim.x) {
+    const long long op = gate_ops[g];
+    if (op < 0) {
+      grad[g] = __longlong_as_double(0x7ff8000000000000LL);  // quiet NaN: no op of its own
+      continue;
+    }
+    double t = 0.0;
+    for (int b = 0; b < grid; ++b) t = __dadd_rn(t, grad_part[(u64)op * grid + b]);
+    grad[g] = t;
+  }
+}
+
 template <int W>
 __global__ void rebuild_kernel(const u64* keys, u64 N, u64* table, u64 mask, u32* error) {
   for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (u64)gridDim.x * blockDim.x) {
@@ -924,6 +1091,37 @@ cudaError_t launch_batch_sweep(const SweepArgs* args, const u32* block_inst, int
 }
 
 template <int W, int ALG>
+cudaError_t launch_adjoint(const AdjointArgs& a, int grid, cudaStream_t s) {
+  AdjointArgs args = a;
+  void* params[] = {&args};
+  return cudaLaunchCooperativeKernel((const void*)adjoint_kernel<W, ALG>, dim3(grid), dim3(BLOCK), params, 0, s);
+}
+
+template <int W, int ALG>
+cudaError_t launch_adjoint_seed(const ExpectArgs& a, const u64* keys, u64 n, double* lam, cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  const int threads = 256;
+  const u64 blocks = (n + threads - 1) / threads;
+  adjoint_seed_kernel<W, ALG><<<(unsigned)(blocks < 65535 ? blocks : 65535), threads, 0, s>>>(a, keys, n, lam);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grad_reduce(const double* grad_part, int grid, const long long* gate_ops, u64 n_gates,
+                               double* grad, cudaStream_t s) {
+  if (!n_gates) return cudaSuccess;
+  const u64 blocks = (n_gates + 255) / 256;
+  grad_reduce_kernel<<<(unsigned)(blocks < 65535 ? blocks : 65535), 256, 0, s>>>(grad_part, grid, gate_ops, n_gates,
+                                                                                  grad);
+  return cudaGetLastError();
+}
+
+template <int W, int ALG>
+int adjoint_grid() {
+  static int sms = 0, per_sm = 0;
+  return co_resident_grid(adjoint_kernel<W, ALG>, 0, &sms, &per_sm);
+}
+
+template <int W, int ALG>
 cudaError_t launch_expect(const ExpectArgs& a, const u64* keys, const double* coeffs, u64 n,
                           ExpectPartial* partials, int grid, cudaStream_t s) {
   expect_kernel<W, ALG><<<grid, BLOCK, 0, s>>>(a, keys, coeffs, n, partials);
@@ -956,6 +1154,9 @@ cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const
   template int batch_grid<Wv, Av>(int);                                                                    \
   template cudaError_t launch_sweep<Wv, Av>(const SweepArgs&, int, cudaStream_t);                       \
   template cudaError_t launch_batch_sweep<Wv, Av>(const SweepArgs*, const u32*, int, cudaStream_t);     \
+  template cudaError_t launch_adjoint<Wv, Av>(const AdjointArgs&, int, cudaStream_t);                   \
+  template cudaError_t launch_adjoint_seed<Wv, Av>(const ExpectArgs&, const u64*, u64, double*, cudaStream_t); \
+  template int adjoint_grid<Wv, Av>();                                                                  \
   template cudaError_t launch_expect<Wv, Av>(const ExpectArgs&, const u64*, const double*, u64,         \
                                              ExpectPartial*, int, cudaStream_t);
 #define PQ_INSTANTIATE_W(Wv)                                                                            \

@@ -71,6 +71,40 @@ struct SweepArgs {
   u32 blk_begin, blk_count;  // blocks of a batched launch that run this instance
   u32* idle_blocks;          // batched: blocks whose instance has left the launch (null: never yield)
   u32 yield_at;              // ... stop at the next op boundary once this many are idle
+  // Recording for the adjoint (null: off).  Per op, from element rec_off[op]:
+  // gate / phase ops store each anticommuting pre-op row's coefficient
+  // (rec_coef) and the post-op row its sin branch went to, or REC_NONE
+  // (rec_idx); a reclaim stores each row's new index or REC_NONE (rec_idx)
+  // and its pre-op keys from row rec_key_off[op] of rec_keys.
+  u32* rec_idx;
+  double* rec_coef;
+  u64* rec_keys;
+  const u64* rec_off;
+  const u64* rec_key_off;
+};
+
+constexpr u32 REC_NONE = 0xffffffffu;
+
+// The reverse sweep of the adjoint over ops [op_begin, op_end) of one
+// recorded segment, last op first.  lam[cur0] holds dE/dc of the rows after
+// op_end - 1; each op maps it to dE/dc of its input rows in the other buffer,
+// and its dE/d(angle) partial of every block goes to grad_part[op * grid + block].
+struct AdjointArgs {
+  const OpDesc* ops;
+  const void* gates;
+  const double* tables;
+  u32 table_len;
+  u32 n_units;
+  u32 op_begin, op_end;
+  u32 cur0;
+  const u64* n_in;               // rows entering each op
+  const u32* rec_idx;
+  const double* rec_coef;
+  const u64* rec_off;
+  const u64* const* key_src;     // per op: keys of its input rows
+  double* lam[2];
+  double* grad_part;
+  SweepState* st;                // barrier only
 };
 
 struct ExpectArgs {
@@ -104,6 +138,19 @@ template <int WM, int ALG>
 int batch_grid(int blocks_per_sm);
 template <int WM, int ALG>
 cudaError_t launch_batch_sweep(const SweepArgs* args, const u32* block_inst, int grid, cudaStream_t s);
+// Cooperative launch of the reverse sweep; grid from adjoint_grid (the
+// co-resident grid), grad_part holds n_ops * grid partials.
+template <int W, int ALG>
+int adjoint_grid();
+template <int W, int ALG>
+cudaError_t launch_adjoint(const AdjointArgs& a, int grid, cudaStream_t s);
+// dE/dc of every row: sign * <s|frame(K)|s>, the seed of the reverse sweep.
+template <int W, int ALG>
+cudaError_t launch_adjoint_seed(const ExpectArgs& a, const u64* keys, u64 n, double* lam, cudaStream_t s);
+// grad[g] = sum over blocks of grad_part[op * grid + b] for op = gate_ops[g]
+// (NaN where gate_ops[g] < 0), in block order.
+cudaError_t launch_grad_reduce(const double* grad_part, int grid, const long long* gate_ops, u64 n_gates,
+                               double* grad, cudaStream_t s);
 template <int W, int ALG>
 cudaError_t launch_expect(const ExpectArgs& a, const u64* keys, const double* coeffs, u64 n,
                           ExpectPartial* partials, int grid, cudaStream_t s);

@@ -16,7 +16,10 @@ from .circuits import (
     PauliCircuit,
     majorana_cp,
     majorana_xx_plus_yy,
+    pauli_cx,
     pauli_rx,
+    pauli_ry,
+    pauli_rz,
     pauli_rzz,
 )
 from .datatypes import MajoranaMonomial, MajoranaTermSum, PauliString, PauliTermSum
@@ -158,3 +161,36 @@ def kicked_ising_batch(n_instances: int = 64, seed: int = 0, n_range=(40, 100), 
         wl.meta.update({"index": i, "site": site, "min_coeff": cut})
         out.append(wl)
     return out
+
+
+def hardware_efficient(n: int = 50, layers: int = 12, seed: int = 0, sigma: float = 0.1, max_weight=8,
+                       min_coeff=1e-5):
+    """Hardware-efficient ansatz: per layer RY(theta) on every qubit, RZ(theta)
+    on every qubit, then a CNOT ladder (q, q+1) for q = 0..n-2 (each CNOT as
+    Z_c(pi/2), X_t(pi/2), Z_c X_t(-pi/2)); one circuit layer per ansatz layer.
+    2 n layers angles ~ N(0, sigma) from numpy.random.default_rng(seed).
+    Observable sum_i Z_i Z_i+1; state |0...0>; no noise.
+
+    meta["param_index"][k] is the angle index of rotation k (circuit order), or
+    -1 for the fixed CNOT pieces; meta["theta"] holds the angles."""
+    rng = np.random.default_rng(seed)
+    theta = rng.normal(0.0, sigma, size=2 * n * layers)
+    circ_layers, pidx = [], []
+    k = 0
+    for _ in range(layers):
+        rots = []
+        for gate in (pauli_ry, pauli_rz):
+            for q in range(n):
+                rots += gate(q, float(theta[k]), n)
+                pidx.append(k)
+                k += 1
+        for q in range(n - 1):
+            cx = pauli_cx(q, q + 1, n)
+            rots += cx
+            pidx += [-1] * len(cx)
+        circ_layers.append(rots)
+    obs = PauliTermSum()
+    for i in range(n - 1):
+        obs.add(PauliString(0, (1 << i) | (1 << (i + 1)), n), 1.0)
+    return Workload(f"hea_{n}q_{layers}l", 0, n, obs, PauliCircuit(circ_layers), max_weight, min_coeff,
+                    meta={"seed": seed, "layers": layers, "theta": theta, "param_index": np.array(pidx)})

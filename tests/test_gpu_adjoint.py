@@ -1,0 +1,172 @@
+"""The adjoint gradient (pq_run_adjoint / propaq_b200.adjoint) on the GPU.
+
+  - exact: without truncation the gradient is the exact derivative, checked
+    against a dense-statevector shift rule (Clifford rotations included: they
+    are deferred into the frame and conjugate every later generator);
+  - frozen decisions: with truncation, noise, phase-only rotations and a
+    TermBudget floor it matches the forward-mode reference, which carries
+    derivatives through the same decisions;
+  - checkpointing changes memory, not results: every segment length gives
+    bit-identical gradients;
+  - the full config: central finite differences on 20 seeded angles.
+"""
+
+import math
+
+import numpy as np
+import pytest
+from adjoint_ref import propagate_with_tangents
+from harness import from_circuit, from_workload, make_cfg
+from test_adjoint_cpu import dense_gradient, random_circuit
+
+import propaq_b200 as pq
+from propaq_b200 import workloads
+from propaq_b200.adjoint import ParametrizedExpectation, _heisenberg_order
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_grad(engine, p, checkpoint_layers=0):
+    cfg, keep = make_cfg(p, want_terms=False)
+    res, nt, g = engine.run_adjoint(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag,
+                                    checkpoint_layers=checkpoint_layers)
+    return res, nt, g
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_gradient_is_exact_without_truncation(gpu_engine, seed):
+    n = 5
+    obs, circ, state = random_circuit(seed, n, 30, clifford=True)
+    p = from_circuit(0, n, obs, circ, state)
+    res, _, g = gpu_grad(gpu_engine, p, checkpoint_layers=2)
+    order = _heisenberg_order(circ)
+    want = dense_gradient(obs, circ, state, n)[order]
+    cliff = np.abs(np.cos(p.angles)) < 1e-9
+    assert np.all(np.isnan(g[cliff])), "deferred Clifford rotations have no gradient entry"
+    np.testing.assert_allclose(g[~cliff], want[~cliff], atol=1e-10)
+
+
+CASES = [
+    dict(max_weight=3, min_coeff=1e-3),
+    dict(max_weight=4, min_coeff=1e-2, noise=0.02),
+    dict(min_coeff=3e-3, min_terms=8),
+    dict(max_weight=3, noise_layered=True),
+    dict(min_coeff=1e-3, phase=True),
+]
+
+
+@pytest.mark.parametrize("seed", range(3))
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+def test_gradient_matches_forward_mode_reference(gpu_engine, oracle, case, seed):
+    case = dict(case)
+    noise = case.pop("noise", None)
+    layered = case.pop("noise_layered", False)
+    phase = case.pop("phase", False)
+    n = 7
+    obs, circ, state = random_circuit(100 + seed, n, 48)
+    if phase:  # two rotations with |sin| < 1e-9: phase-only ops
+        circ.layers[1][0].angle = 1e-11
+        circ.layers[3][2].angle = -2e-10
+    p = from_circuit(0, n, obs, circ, state, **case)
+    if noise:
+        p.noise_table = np.array([math.exp(-noise * w) for w in range(n + 1)])
+    if layered:
+        L = len(p.offsets) - 1
+        p.noise_tables_layered = np.array([[math.exp(-0.01 * (l + 1) * w) for w in range(n + 1)] for l in range(L)])
+    e_ref, g_ref = propagate_with_tangents(oracle, p)
+    res, _, g = gpu_grad(gpu_engine, p, checkpoint_layers=3)
+    assert abs(res.expectation_value - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
+    scale = max(1.0, float(np.abs(g_ref).max()))
+    np.testing.assert_allclose(g, g_ref, rtol=1e-9, atol=1e-12 * scale)
+
+
+def test_checkpoint_segments_do_not_change_the_gradient(gpu_engine):
+    wl = workloads.hardware_efficient(12, 5, seed=2)
+    p = from_workload(wl)
+    ref = gpu_grad(gpu_engine, p, 0)
+    for c in (1, 2, 3, 4, 7):
+        res, nt, g = gpu_grad(gpu_engine, p, c)
+        assert res.expectation_value == ref[0].expectation_value
+        assert np.array_equal(nt, ref[1])
+        assert np.array_equal(np.isnan(g), np.isnan(ref[2]))
+        ok = ~np.isnan(g)
+        assert np.array_equal(g[ok], ref[2][ok]), f"checkpoint_layers={c}"
+
+
+def test_forward_part_equals_plain_run(gpu_engine):
+    wl = workloads.kicked_ising(5, 6, 4)
+    p = from_workload(wl)
+    cfg, keep = make_cfg(p, want_terms=False)
+    plain, nt_plain = gpu_engine.run(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag)
+    res, nt, g = gpu_grad(gpu_engine, p, 2)
+    assert res.expectation_value == plain.expectation_value
+    assert np.array_equal(nt, nt_plain)
+    assert np.isfinite(g[np.abs(np.cos(p.angles)) >= 1e-9]).all()
+
+
+def test_torch_autograd_function(gpu_engine):
+    import torch
+
+    wl = workloads.hardware_efficient(10, 3, seed=4)
+    spec = ParametrizedExpectation(pq.PauliPropagator(truncation=wl.truncation()), wl.observable, wl.circuit,
+                                   wl.meta["param_index"], checkpoint_layers=1)
+    theta = torch.tensor(wl.meta["theta"], dtype=torch.float64, device="cuda", requires_grad=True)
+    loss = 3.0 * spec(theta)
+    loss.backward()
+    e, g = spec.value_and_grad(wl.meta["theta"])
+    assert float(loss.detach()) == pytest.approx(3.0 * e, rel=1e-15)
+    np.testing.assert_array_equal(theta.grad.cpu().numpy(), 3.0 * g)
+    with torch.no_grad():
+        assert float(spec(theta)) == e
+
+
+def test_parameter_shift_agrees_without_truncation(gpu_engine):
+    wl = workloads.hardware_efficient(8, 2, seed=5, max_weight=None, min_coeff=None)
+    spec = ParametrizedExpectation(pq.PauliPropagator(), wl.observable, wl.circuit, wl.meta["param_index"])
+    _, g = spec.value_and_grad(wl.meta["theta"])
+    np.testing.assert_allclose(spec.parameter_shift(wl.meta["theta"], batch=8), g, atol=1e-11)
+
+
+def test_config_hardware_efficient_finite_differences(gpu_engine):
+    # 50 qubits, 12 layers, 1200 angles, w <= 8, |c| >= 1e-5: central
+    # differences on 20 seeded angles.  A difference quotient that straddles a
+    # truncation decision (a term crossing the cutoff within +-h) jumps by
+    # about cutoff / h, so h starts at 1e-5 and shrinks (1e-6, 1e-7) while any
+    # per-gate live count at theta +- h differs from theta's.
+    from propaq_b200 import _native
+
+    wl = workloads.hardware_efficient()
+    spec = ParametrizedExpectation(pq.PauliPropagator(truncation=wl.truncation()), wl.observable, wl.circuit,
+                                   wl.meta["param_index"], checkpoint_layers=3)
+    th = wl.meta["theta"]
+    e, g = spec.value_and_grad(th)
+
+    def run(t):
+        res, nt = _native.engine(0).run(*spec._call_args(t))
+        return res.expectation_value, nt
+
+    e0, nt0 = run(th)
+    assert e0 == e
+    picks = np.random.default_rng(0).choice(len(th), size=20, replace=False)
+    bad = []
+    for k in picks:
+        for h in (1e-5, 1e-6, 1e-7):
+            tp, tm = th.copy(), th.copy()
+            tp[k] += h
+            tm[k] -= h
+            (ep, ntp), (em, ntm) = run(tp), run(tm)
+            if np.array_equal(ntp, nt0) and np.array_equal(ntm, nt0):
+                break
+        fd = (ep - em) / (2 * h)
+        tol = 1e-5 * abs(g[k]) + 64 * np.finfo(float).eps * abs(e) / h
+        if not abs(fd - g[k]) <= tol:
+            bad.append((int(k), h, float(g[k]), fd))
+    assert not bad, f"adjoint vs central differences (angle, h, adjoint, fd): {bad}"
+
+
+def test_gradient_refusals(gpu_engine):
+    wl = workloads.kicked_ising(4, 4, 2)  # RZZ(-pi/2) changes weight
+    p = from_workload(wl)
+    p.min_terms = 10
+    with pytest.raises(NotImplementedError, match="TermBudget"):
+        gpu_grad(gpu_engine, p)
