@@ -22,6 +22,11 @@ kicked-Ising instances of 40..100 qubits (4 noise scales x 4 coefficient
 cutoffs x 4 observable sites) in shared persistent launches (pq_run_batch),
 beside the same 64 instances as sequential pq_run calls on the same GPU.
 
+`--workload adjoint` times the full gradient of a 50-qubit, 12-layer
+hardware-efficient ansatz (1200 angles, sum of Z_i Z_i+1, w <= 8,
+|c| >= 1e-5) through the adjoint pass, beside a timed sample of the
+2400-evaluation parameter-shift gradient (batched propagations) on the same GPU.
+
 `--impl reference` times the CPU restatement of the reference engine (the
 oracle) on the host cores instead.  With torchrun (N > 1) every rank runs an
 independent replica of the workload (the path does not shard).
@@ -52,13 +57,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "majorana", "majorana_small", "tfim", "batch"])
+    ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "majorana", "majorana_small", "tfim", "batch", "adjoint"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="sweep blocks per SM (0 = as many as fit)")
     ap.add_argument("--split", type=int, default=1, help="batch: 0 equal grid shares, 1 by remaining work")
     ap.add_argument("--rebalance-pct", type=int, default=25, help="batch: re-split when this %% of the grid idles")
     ap.add_argument("--no-sequential", action="store_true", help="batch: skip the sequential pq_run comparison")
+    ap.add_argument("--checkpoint-layers", type=int, default=3, help="adjoint: layers per checkpoint segment")
+    ap.add_argument("--shift-sample", type=int, default=96, help="adjoint: parameter-shift evaluations timed")
     return ap.parse_args()
 
 
@@ -357,6 +364,133 @@ def main_batch(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def main_adjoint(args, world, rank, local):
+    """The ansatz gradient.  value = full gradients per second of device time
+    (forward + reverse pass)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from harness import from_workload, run_oracle
+
+    from propaq_b200 import PauliPropagator, workloads
+    from propaq_b200.adjoint import ParametrizedExpectation
+
+    wl = workloads.hardware_efficient()
+    th = wl.meta["theta"]
+    desc = ("hardware-efficient ansatz 50 qubits, 12 layers of RY+RZ on all + CNOT ladder (Z_c(pi/2), X_t(pi/2), "
+            "Z_cX_t(-pi/2)), 1200 angles ~ N(0,0.1), sum Z_i Z_i+1, |0..0>, w<=8, |c|>=1e-5, no noise")
+    cores = os.cpu_count() or 1
+    base_line = {"metric": "gradients/s", "unit": "gradients/s", "n_gpus": args.gpus, "steps": args.steps,
+                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                 "dtype": "f64", "data": "synthetic (seeded; no dataset)",
+                 "config": {"workload": desc, "name": wl.name, "n_units": 50, "angles": len(th),
+                            "gates": len(wl.circuit.rotations), "checkpoint_layers": args.checkpoint_layers,
+                            "parallelism": f"replicas x{world}", "l2": "flushed between steps"}}
+    spec_cpu = ParametrizedExpectation(PauliPropagator(truncation=wl.truncation()), wl.observable, wl.circuit,
+                                       wl.meta["param_index"])
+    n_shift = 2 * len(spec_cpu._param_gates)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # The reference has no gradient: its CPU arm is the parameter-shift rule
+        # on the oracle, timed on a bounded sample of evaluations.
+        o = oracle_load()
+        p = from_workload(wl)
+        base = spec_cpu._call_args(th)
+        n_eval, t0 = 0, time.perf_counter()
+        while n_eval < 2 or time.perf_counter() - t0 < args.cpu_seconds:
+            g = spec_cpu._param_gates[(n_eval // 2) % len(spec_cpu._param_gates)]
+            p.angles = base[4].copy()
+            p.angles[g] += (1 if n_eval % 2 == 0 else -1) * math.pi / 2
+            run_oracle(o, p, n_partitions=cores, want_terms=False)
+            n_eval += 1
+        el = time.perf_counter() - t0
+        per_grad = el / n_eval * n_shift
+        v = 1.0 / per_grad
+        line = dict(base_line, impl="reference", value=v, ms_per_step=1e3 * per_grad,
+                    cpu_baseline={"value": v, "unit": "gradients/s", "cores": cores, "kind": "port",
+                                  "sample": f"{n_eval} parameter-shift evaluations in {el:.1f} s on the oracle "
+                                            f"({cores} threads), scaled to {n_shift}"},
+                    e2e={"value": v, "unit": "gradients/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    from propaq_b200 import _native
+
+    torch.cuda.set_device(local)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    prop = PauliPropagator(truncation=wl.truncation(), device=local)
+    spec = ParametrizedExpectation(prop, wl.observable, wl.circuit, wl.meta["param_index"],
+                                   checkpoint_layers=args.checkpoint_layers)
+    theta = torch.tensor(th, dtype=torch.float64)
+
+    def settle():
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier(world)
+
+    for _ in range(args.warmup):
+        settle()
+        spec.value_and_grad(th)
+    dev_ms = fwd_ms = 0.0
+    launches = 0
+    e2e_s = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            settle()
+            spec.value(th)
+            fwd_ms += prop.last_run.device_ms
+            settle()
+            e, g = spec.value_and_grad(th)
+            dev_ms += prop.last_run.device_ms
+            launches += int(prop.last_run.gpu_launches)
+        for _ in range(args.steps):
+            settle()
+            t0 = time.perf_counter()
+            th_req = theta.clone().requires_grad_(True)
+            spec(th_req).backward()
+            _ = th_req.grad.numpy().sum()
+            e2e_s += time.perf_counter() - t0
+        # Parameter shift: a timed sample of its 2 x 1200 propagations, 8 at a
+        # time through pq_run_batch, scaled to the full count.
+        base = spec._call_args(th)
+        eng = _native.engine(local)
+        items = []
+        for k in range(args.shift_sample):
+            gi = spec._param_gates[(k // 2) % len(spec._param_gates)]
+            a = base[4].copy()
+            a[gi] += (1 if k % 2 == 0 else -1) * math.pi / 2
+            items.append(tuple(base[:4]) + (a,) + tuple(base[5:]))
+        settle()
+        ps_ms = 0.0
+        for i in range(0, len(items), 8):
+            out = eng.run_batch(items[i:i + 8], want_n_terms=False)
+            ps_ms += out[0][0].device_ms
+    clocks = clk.summary()
+    dev_s = max_over_ranks(world, dev_ms / 1e3)
+    e2e_s = max_over_ranks(world, e2e_s)
+    shift_ms = ps_ms / len(items) * n_shift
+    h2d = sum(int(np.asarray(x).nbytes) for x in base[1:] if x is not None) + 8 * len(th)
+    line = dict(base_line, value=world * args.steps / dev_s, ms_per_step=1e3 * dev_s / args.steps,
+                forward_ms=fwd_ms / args.steps, expectation_value=e,
+                e2e={"value": world * args.steps / e2e_s, "unit": "gradients/s", "h2d_bytes_per_step": int(h2d),
+                     "d2h_bytes_per_step": 8 * len(spec._fixed) * 2, "ms_per_step": 1e3 * e2e_s / args.steps,
+                     "path": "torch.autograd: ParametrizedExpectation(theta).backward()"},
+                gpu_launches=launches // max(1, args.steps),
+                parameter_shift={"evaluations": n_shift, "timed_sample": len(items),
+                                 "ms_per_evaluation": ps_ms / len(items), "ms_per_gradient": shift_ms,
+                                 "how": "pq_run_batch, 8 shifted circuits per call, device time",
+                                 "adjoint_speedup": shift_ms / (1e3 * dev_s / args.steps)},
+                roofline=None, clocks=clocks)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def oracle_load():
     sys.path.insert(0, str(ROOT / "tests"))
     from oracle_client import Oracle
@@ -369,6 +503,8 @@ def main():
     world, rank, local = dist_setup()
     if args.workload == "batch":
         return main_batch(args, world, rank, local)
+    if args.workload == "adjoint":
+        return main_adjoint(args, world, rank, local)
     wl, desc = make_workload(args.workload)
     cores = os.cpu_count() or 1
     W = 1
