@@ -48,7 +48,6 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr long LOOKBACK_SPIN_LIMIT = 1L << 22;  // ~0.3 s with the backoff below
 constexpr long BARRIER_SPIN_LIMIT = 1L << 25;   // ~2 s with the backoff below
 constexpr u32 BAR_GROUPS = SweepState::BAR_GROUPS;
-constexpr int TILE_LARGE = BLOCK * MAX_ITEMS;
 
 enum : int { S_EMIT = 0, S_HELD = 1, S_DROP = 2 };
 
@@ -69,37 +68,82 @@ struct Grp {
 // group arrives on the top counter, and the last top arrival releases
 // everyone by bumping the generation.  Every wait is bounded; once one
 // expires, ERR_BARRIER_TIMEOUT makes every later barrier fall through.
+// The three steps run on thread 0 of each block, after a fence.
+
+// Arrives; true for the last arrival of the whole grid.
+__device__ __forceinline__ bool barrier_arrive(SweepState* st, const Grp g_) {
+  const u32 nb = g_.nblk;
+  const u32 grp = g_.bid % BAR_GROUPS;
+  const u32 in_grp = nb / BAR_GROUPS + (grp < nb % BAR_GROUPS ? 1u : 0u);
+  const u32 n_grp = nb < BAR_GROUPS ? nb : BAR_GROUPS;
+  if (atomicAdd(&st->bar_group[grp].count, 1u) != in_grp - 1) return false;
+  st->bar_group[grp].count = 0;
+  return atomicAdd(&st->bar_count, 1u) == n_grp - 1;
+}
+__device__ __forceinline__ void barrier_release(SweepState* st, u32 g) {
+  st->bar_count = 0;
+  __threadfence();
+  atomicExch(&st->bar_gen, g + 1);
+}
+__device__ __forceinline__ void barrier_wait(SweepState* st, u32 g) {
+  long spins = 0;
+  while (*(volatile u32*)&st->bar_gen == g) {
+    if (*(volatile u32*)&st->error & ERR_BARRIER_TIMEOUT) break;
+    if (++spins > BARRIER_SPIN_LIMIT) {
+      atomicOr(&st->error, ERR_BARRIER_TIMEOUT);
+      break;
+    }
+    __nanosleep(20);
+  }
+}
+
 __device__ __forceinline__ void grid_barrier(SweepState* st, u32& gen, const Grp g_) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    const u32 g = gen;
-    const u32 nb = g_.nblk;
-    const u32 grp = g_.bid % BAR_GROUPS;
-    const u32 in_grp = nb / BAR_GROUPS + (grp < nb % BAR_GROUPS ? 1u : 0u);
-    const u32 n_grp = nb < BAR_GROUPS ? nb : BAR_GROUPS;
-    bool last = false;
-    if (atomicAdd(&st->bar_group[grp].count, 1u) == in_grp - 1) {
-      st->bar_group[grp].count = 0;
-      last = atomicAdd(&st->bar_count, 1u) == n_grp - 1;
-    }
-    if (last) {
-      st->bar_count = 0;
-      __threadfence();
-      atomicExch(&st->bar_gen, g + 1);
-    } else {
-      long spins = 0;
-      while (*(volatile u32*)&st->bar_gen == g) {
-        if (*(volatile u32*)&st->error & ERR_BARRIER_TIMEOUT) break;
-        if (++spins > BARRIER_SPIN_LIMIT) {
-          atomicOr(&st->error, ERR_BARRIER_TIMEOUT);
-          break;
-        }
-        __nanosleep(20);
-      }
-    }
-    gen = g + 1;
+    if (barrier_arrive(st, g_))
+      barrier_release(st, gen);
+    else
+      barrier_wait(st, gen);
+    ++gen;
     __threadfence();
+  }
+  __syncthreads();
+}
+
+// What every block needs after the end-of-op barrier, read once by thread 0.
+struct OpShared {
+  u64 n;            // live rows entering the next op
+  u32 err;          // SweepState::error
+  u32 yield_after;  // SweepState::yield_after
+};
+
+// The barrier between two ops of a sweep.  Thread 0 of each block, once it
+// has arrived (or released), runs prefetch() -- loading the next op's
+// descriptors, which do not depend on this op, while it waits -- and after
+// the release reads the next op's live count and the error / yield words
+// together into shared memory, one round trip for the block.
+template <class Prefetch>
+__device__ __forceinline__ void op_barrier(SweepState* st, u32& gen, const Grp g_, const u64* n_next, OpShared& os,
+                                           Prefetch prefetch) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (barrier_arrive(st, g_)) {
+      barrier_release(st, gen);
+      prefetch();
+    } else {
+      prefetch();
+      barrier_wait(st, gen);
+    }
+    ++gen;
+    __threadfence();
+    const u64 n = ld_volatile(n_next);
+    const u32 e = *(volatile u32*)&st->error;
+    const u32 y = *(volatile u32*)&st->yield_after;
+    os.n = n;
+    os.err = e;
+    os.yield_after = y;
   }
   __syncthreads();
 }
@@ -215,6 +259,29 @@ __device__ void insert(const u64* q, u64 row, u64* table, u64 mask, u32* error) 
     i = (i + 1) & mask;
   }
   atomicOr(error, ERR_PROBE_OVERFLOW);
+}
+
+// Claims a slot for q before its row is known: the slot holds q's
+// fingerprint and the placeholder row PENDING_ROW (never below a lookup's
+// n_pre, so no lookup of the running op can match it) until set_row writes
+// the row into its low half.  Claiming early lets the atomic round trip
+// overlap the tile scan.  Returns the slot, or NO_SLOT if the table is full.
+constexpr u32 PENDING_ROW = 0xfffffffeu;
+constexpr u64 NO_SLOT = ~0ULL;
+template <int W>
+__device__ u64 claim_slot(const u64* q, u64* table, u64 mask, u32* error) {
+  const u64 h = key_hash<W>(q);
+  const u64 v = ((h >> 32) << 32) | PENDING_ROW;
+  u64 i = bucket_start(h, mask);
+  for (u64 probe = 0; probe <= mask; ++probe) {
+    if (__ldcg(table + i) == EMPTY_SLOT && atomicCAS(table + i, EMPTY_SLOT, v) == EMPTY_SLOT) return i;
+    i = (i + 1) & mask;
+  }
+  atomicOr(error, ERR_PROBE_OVERFLOW);
+  return NO_SLOT;
+}
+__device__ __forceinline__ void set_row(u64* table, u64 slot, u64 row) {
+  if (slot != NO_SLOT) reinterpret_cast<u32*>(table + slot)[0] = (u32)row;  // little-endian low half
 }
 
 // Row holding q among the pre-gate rows, or -1: the key's first bucket is
@@ -381,6 +448,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
     }
     u32 emit = 0;
     double bval[IT];
+    u64 slot[IT];
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
       bval[k] = 0.0;
@@ -396,6 +464,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
         if (si == S_EMIT) {
           emit |= 1u << k;
           bval[k] = bi;
+          slot[k] = claim_slot<W>(q, a.table, a.table_mask, &st->error);
         }
         if (a.rec_idx) record_single(a, op, r, c[k]);
       } else {
@@ -428,7 +497,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
       for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ g.gen[w];
       store_key<W>(keys, row, q);
       coeffs[row] = bval[k];
-      insert<W>(q, row, a.table, a.table_mask, &st->error);
+      set_row(a.table, slot[k], row);
       if (a.rec_idx) a.rec_idx[a.rec_off[op] + (u64)t * TL + (u64)k * BLOCK + threadIdx.x] = (u32)row;
     }
     __syncthreads();  // sm is reused by the next tile
@@ -607,6 +676,7 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
     u32 keep = 0;
     double cv[IT];
     u64 key[IT][W];
+    u64 slot[IT];
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
       const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
@@ -625,6 +695,7 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
       const bool kp = (a.max_weight == NO_WEIGHT_CUT || w <= a.max_weight) &&
                       (!a.has_min_coeff || fabs(c) >= a.min_coeff);
       keep |= (u32)kp << k;
+      if (kp) slot[k] = claim_slot<W>(key[k], a.table, a.table_mask, &st->error);
       if (a.rec_idx) {
         a.rec_idx[a.rec_off[op] + r] = REC_NONE;
         store_key<W>(a.rec_keys + a.rec_key_off[op] * W, r, key[k]);
@@ -639,7 +710,7 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
       const u64 row = sm.excl + sm.cnt[k * NWARPS + warp] + __popc(masks[k] & lt);
       store_key<W>(keys_out, row, key[k]);
       coeffs_out[row] = cv[k];
-      insert<W>(key[k], row, a.table, a.table_mask, &st->error);
+      set_row(a.table, slot[k], row);
       if (a.rec_idx) a.rec_idx[a.rec_off[op] + (u64)t * TL + (u64)k * BLOCK + threadIdx.x] = (u32)row;
     }
     __syncthreads();
@@ -650,14 +721,27 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
 template <int W, int ALG>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   __shared__ TileSmem sm;
-  __shared__ GateDesc<W> sgate;
+  __shared__ GateDesc<W> sgate[2];  // op k's generator in slot k & 1
+  __shared__ OpDesc sod[2];
+  __shared__ OpShared os;
   SweepState* st = a.st;
   u32 gen = *(volatile u32*)&st->bar_gen;
   int cur = (int)a.cur0;
   u32 op = a.op_begin;
+  auto fetch_op = [&](u32 k) {  // thread 0
+    if (k >= a.op_end) return;
+    const OpDesc d = a.ops[k];
+    sod[k & 1] = d;
+    if (d.kind == OP_GATE || d.kind == OP_PHASE) sgate[k & 1] = reinterpret_cast<const GateDesc<W>*>(a.gates)[d.idx];
+  };
+  if (threadIdx.x == 0) {
+    fetch_op(op);
+    os.n = ld_volatile(&st->n[op & 1]);
+  }
+  __syncthreads();
   for (; op < a.op_end; ++op) {
-    const OpDesc od = a.ops[op];
-    const u64 N = ld_volatile(&st->n[op & 1]);
+    const OpDesc od = sod[op & 1];
+    const u64 N = os.n;
     u64* keys = a.keys[cur];
     double* coeffs = a.coeffs[cur];
     if (od.kind == OP_GATE || od.kind == OP_PHASE) {
@@ -665,12 +749,10 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
         if (grp.bid == 0 && threadIdx.x == 0) st->halt = op;
         break;
       }
-      if (threadIdx.x == 0) sgate = reinterpret_cast<const GateDesc<W>*>(a.gates)[od.idx];
-      __syncthreads();
       if (od.kind == OP_GATE) {
-        gate_op<W, ALG>(a, sgate, op, N, keys, coeffs, sm, grp);
+        gate_op<W, ALG>(a, sgate[op & 1], op, N, keys, coeffs, sm, grp);
       } else {
-        phase_op<W, ALG>(a, sgate, op, N, keys, coeffs, grp);
+        phase_op<W, ALG>(a, sgate[op & 1], op, N, keys, coeffs, grp);
         if (grp.bid == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
       }
     } else if (od.kind == OP_NOISE_SCALE) {
@@ -688,17 +770,16 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     // this op boundary so that the host can hand the idle blocks to the
     // instances still running.  Block 0 names the op before the barrier and
     // every block compares it with its own op after it, so all blocks take
-    // the same branch (a block still reading after an earlier barrier sees a
-    // different op and goes on).
+    // the same branch (a block reading late sees a later op and goes on).
     if (a.idle_blocks && grp.bid == 0 && threadIdx.x == 0 && *(volatile u32*)a.idle_blocks >= a.yield_at)
       *(volatile u32*)&st->yield_after = op + 1;
-    grid_barrier(st, gen, grp);
-    if (*(volatile u32*)&st->error) {
+    op_barrier(st, gen, grp, &st->n[(op + 1) & 1], os, [&] { fetch_op(op + 1); });
+    if (os.err) {
       ++op;
       break;
     }
     if (grp.bid == 0 && threadIdx.x == 0) {
-      const u64 n_new = ld_volatile(&st->n[(op + 1) & 1]);
+      const u64 n_new = os.n;
       a.hist[op] = n_new;
       if (n_new > st->peak) st->peak = n_new;
       if (a.stamps) {
@@ -707,7 +788,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
         a.stamps[op] = t;
       }
     }
-    if (a.idle_blocks && *(volatile u32*)&st->yield_after == op + 1) {
+    if (a.idle_blocks && os.yield_after == op + 1) {
       ++op;
       break;
     }
