@@ -814,6 +814,27 @@ int build_ops(Plan& P, NeedN need_n) {
   return PQ_OK;
 }
 
+// Marks consecutive rotation ops whose (frame-conjugated) generators commute
+// as fused pairs, OP_GATE2 + OP_GATE2_TAIL, which the sweep runs in one pass
+// (gate2_tiles).  Not with a TermBudget floor: its lossless switch reads the
+// live count between the two rotations.  The reverse sweep of the adjoint
+// needs each rotation's own record, so its runs do not fuse.
+void fuse_pairs(Plan& P) {
+  if (P.has_floor) return;
+  const size_t gw = gdesc_words(P.W);
+  for (size_t i = 0; i + 1 < P.ops.size(); ++i) {
+    if (P.ops[i].kind != pq::OP_GATE || P.ops[i + 1].kind != pq::OP_GATE) continue;
+    if (P.ops[i + 1].idx != P.ops[i].idx + 1) continue;
+    const u64* g1 = &P.gdesc[P.ops[i].idx * gw];  // GateDesc starts with the generator's words
+    const u64* g2 = &P.gdesc[P.ops[i + 1].idx * gw];
+    if (host_anticommutes(P.alg, P.W, g1, g2)) continue;
+    if (std::equal(g1, g1 + P.W, g2)) continue;  // one axis twice: the family would be a pair
+    P.ops[i].kind = pq::OP_GATE2;
+    P.ops[i + 1].kind = pq::OP_GATE2_TAIL;
+    ++i;
+  }
+}
+
 // Enqueues the upload of the ops and gate descriptors not yet on the device.
 void upload_ops(pq_engine* E, Slot& S, Plan& P) {
   if (P.ops.size() > P.uploaded_ops) {
@@ -1076,6 +1097,8 @@ int finish(pq_engine* E, Slot& S, Plan& P, const std::vector<pq::ExpectPartial>&
     const double op_ms = i ? (double)(stamps[i] - stamps[i - 1]) * 1e-6 : 0.0;
     switch (P.ops[i].kind) {
       case pq::OP_GATE:
+      case pq::OP_GATE2:
+      case pq::OP_GATE2_TAIL:
         ++res->gate_ops;
         res->gate_ms += op_ms;
         res->sum_rows_gate += n_in;
@@ -1122,6 +1145,7 @@ int run_one(pq_engine* E, const Inputs& in, int W) {
     return PQ_OK;
   };
   if (int rc = build_ops(P, need_n)) return rc;
+  fuse_pairs(P);
   if (int rc = execute_single(E, S, P, grid, &began)) return rc;
   if (!began) cudaEventRecord(E->ev_begin, E->stream);
   std::vector<pq::ExpectPartial> parts;
@@ -1382,6 +1406,7 @@ int run_batch(pq_engine* E, const std::vector<Inputs>& ins, int WM, const pq_bat
     if (int rc = prepare(E, plans[i], ins[i], W)) return rc;
     if (int rc = setup_slot(E, E->slots[i], plans[i])) return rc;
     if (int rc = build_ops(plans[i], no_sync)) return rc;
+    fuse_pairs(plans[i]);
     upload_ops(E, E->slots[i], plans[i]);
   }
   const int grid_max = with_words(WM, [&](auto w) {

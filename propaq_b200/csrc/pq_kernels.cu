@@ -116,6 +116,7 @@ struct OpShared {
   u64 n;            // live rows entering the next op
   u32 err;          // SweepState::error
   u32 yield_after;  // SweepState::yield_after
+  u32 extra;        // a word the op asked for (a fused op's count after its first rotation)
 };
 
 // The barrier between two ops of a sweep.  Thread 0 of each block, once it
@@ -124,8 +125,8 @@ struct OpShared {
 // the release reads the next op's live count and the error / yield words
 // together into shared memory, one round trip for the block.
 template <class Prefetch>
-__device__ __forceinline__ void op_barrier(SweepState* st, u32& gen, const Grp g_, const u64* n_next, OpShared& os,
-                                           Prefetch prefetch) {
+__device__ __forceinline__ void op_barrier(SweepState* st, u32& gen, const Grp g_, const u64* n_next, const u32* extra,
+                                           OpShared& os, Prefetch prefetch) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -141,9 +142,11 @@ __device__ __forceinline__ void op_barrier(SweepState* st, u32& gen, const Grp g
     const u64 n = ld_volatile(n_next);
     const u32 e = *(volatile u32*)&st->error;
     const u32 y = *(volatile u32*)&st->yield_after;
+    const u32 x = extra ? *(const volatile u32*)extra : 0u;
     os.n = n;
     os.err = e;
     os.yield_after = y;
+    os.extra = x;
   }
   __syncthreads();
 }
@@ -388,12 +391,11 @@ __device__ __forceinline__ void record_pair(const SweepArgs& a, u32 op, u64 r, u
 // waits on blocks that are running.
 template <int W, int ALG, int IT>
 __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
-                                           double* coeffs, TileSmem& sm, const Grp grp) {
+                                           double* coeffs, TileSmem& sm, const Grp grp, u64* n_out) {
   using Ops = typename Alg<ALG>::T;
   constexpr int TL = BLOCK * IT;
   SweepState* st = a.st;
   const u32 ntiles = (u32)((N + TL - 1) / TL);
-  u64* n_out = &st->n[(op + 1) & 1];
   // TermBudget: below the floor every lossy predicate is off (termsum.rs:60-76).
   const bool lossless = a.min_terms && N < a.min_terms;
   const u32 wcut = lossless ? NO_WEIGHT_CUT : a.max_weight;
@@ -511,13 +513,12 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
 // thread taking its MAX_ITEMS rows one after the other.
 template <int W, int ALG>
 __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
-                                                 double* coeffs, TileSmem& sm) {
+                                                 double* coeffs, TileSmem& sm, u64* n_out) {
   using Ops = typename Alg<ALG>::T;
   constexpr int IT = MAX_ITEMS;
   constexpr int TL = BLOCK * IT;
   SweepState* st = a.st;
   const u32 ntiles = (u32)((N + TL - 1) / TL);
-  u64* n_out = &st->n[(op + 1) & 1];
   const bool lossless = a.min_terms && N < a.min_terms;
   const u32 wcut = lossless ? NO_WEIGHT_CUT : a.max_weight;
   const bool ccut = !lossless && a.has_min_coeff;
@@ -608,17 +609,184 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
 
 template <int W, int ALG>
 __device__ __forceinline__ void gate_op(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
-                                        double* coeffs, TileSmem& sm, const Grp grp) {
+                                        double* coeffs, TileSmem& sm, const Grp grp, u64* n_out) {
   if (N == 0) {
-    if (grp.bid == 0 && threadIdx.x == 0) st_volatile(&a.st->n[(op + 1) & 1], 0);
+    if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
     return;
   }
   // Few rows: one row per thread and at most one 256-row tile per block, so
   // every row's chain of dependent loads runs at once.
   if (N <= (u64)grp.nblk * BLOCK)
-    gate_tiles<W, ALG, 1>(a, d, op, N, keys, coeffs, sm, grp);
+    gate_tiles<W, ALG, 1>(a, d, op, N, keys, coeffs, sm, grp, n_out);
   else
-    gate_tiles_large<W, ALG>(a, d, op, N, keys, coeffs, sm);
+    gate_tiles_large<W, ALG>(a, d, op, N, keys, coeffs, sm, n_out);
+}
+
+// Two rotations G1 then G2 whose generators commute, in one pass over the
+// rows.  Since G1 G2 = G2 G1, the keys {K, K^G1, K^G2, K^G1^G2} (a family)
+// all anticommute with G1 iff K does and with G2 iff K does, and no rotation
+// moves a term out of its family; so the two sequential steps of the
+// reference -- the pair rule for G1 on (K, K^G1) and (K^G2, K^G1^G2), then
+// for G2 on (K, K^G2) and (K^G1, K^G1^G2) with the results -- can be run for
+// each family by one thread: the present row of lowest index owns the family
+// (rows look up the other members among the rows entering the op), writes the
+// coefficients of its present members and appends the members that either
+// step creates, with their final coefficients.  Every coefficient is the same
+// two-operand result as in two separate passes; only the order in which the
+// new rows are appended differs (deterministic: by owner row, then member).
+// Not used with a TermBudget floor (its lossless switch reads the live count
+// between the two rotations) or when recording for the adjoint.  The sweep
+// runs it when every block has at most one tile (the latency-bound regime it
+// is for); with more rows it runs the two rotations one after the other.
+template <int W, int ALG>
+__device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& d1, const GateDesc<W>& d2, u32 op,
+                                         u64 N, u64* keys, double* coeffs, TileSmem& sm, const Grp grp, u64* n_out) {
+  using Ops = typename Alg<ALG>::T;
+  constexpr int TL = BLOCK;
+  SweepState* st = a.st;
+  const u32 ntiles = (u32)((N + TL - 1) / TL);
+  const u32 wcut = a.max_weight;
+  const bool ccut = a.has_min_coeff != 0;
+  const double minc = a.min_coeff;
+  const u32 epoch = a.epoch_base + op;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  u32 n_anti1 = 0, n_anti2 = 0, n_born1 = 0;
+  for (u32 t = grp.bid; t < ntiles; t += grp.nblk) {
+    const u64 r = (u64)t * TL + threadIdx.x;
+    u64 k0[W];
+    bool a1 = false, a2 = false;
+    if (r < N) {
+      load_key<W>(keys, r, k0);
+      a1 = Ops::template anticommutes<W>(d1.g, k0);
+      a2 = Ops::template anticommutes<W>(d2.g, k0);
+    }
+    n_anti1 += a1;
+    n_anti2 += a2;
+    // key of member m (bit 0: times G1, bit 1: times G2)
+    auto member = [&](int m, u64* out) {
+#pragma unroll
+      for (int w = 0; w < W; ++w) out[w] = k0[w] ^ ((m & 1) ? d1.g.gen[w] : 0ull) ^ ((m & 2) ? d2.g.gen[w] : 0ull);
+    };
+    long long j[4] = {(long long)r, -1, -1, -1};
+    {
+      u64 q[W];
+      if (a1) {
+        member(1, q);
+        j[1] = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+      }
+      if (a2) {
+        member(2, q);
+        j[2] = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+      }
+      if (a1 && a2) {
+        member(3, q);
+        j[3] = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+      }
+    }
+    const bool own = (a1 || a2) && (j[1] < 0 || (u64)j[1] > r) && (j[2] < 0 || (u64)j[2] > r) &&
+                     (j[3] < 0 || (u64)j[3] > r);
+    u32 emit = 0;
+    double bval[3] = {0.0, 0.0, 0.0};
+    if (own) {
+      double c[4];
+      bool p[4];
+      int born[4] = {0, 0, 0, 0};  // the step that created the member (1 or 2), 0 if it entered the op
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        p[m] = j[m] >= 0;
+        c[m] = p[m] ? __ldcg(coeffs + j[m]) : 0.0;
+      }
+      // One reference step on the pair (x, y) of the family
+      // (termsum.rs:604-751): the pair rule if both are present, else the
+      // lone member's cos update and, on EMIT, the other member's creation.
+      auto step = [&](const GateDesc<W>& d, int x, int y, int s) {
+        if (!p[x] && !p[y]) return;
+        u64 kx[W], ky[W];
+        member(x, kx);
+        member(y, ky);
+        auto state = [&](double cv, const u64* ch) -> int {
+          if (ccut && fabs(__dmul_rn(cv, d.sn)) < minc) return S_HELD;
+          if (wcut != NO_WEIGHT_CUT && Ops::template weight<W>(ch, a.n_units) > wcut) return S_DROP;
+          return S_EMIT;
+        };
+        if (p[x] && p[y]) {
+          const double bx = __dmul_rn(__dmul_rn(c[x], d.sn), neg_im(Ops::template product_exp<W>(d.g, kx), d.g.sign));
+          const double by = __dmul_rn(__dmul_rn(c[y], d.sn), neg_im(Ops::template product_exp<W>(d.g, ky), d.g.sign));
+          const int sx = state(c[x], ky), sy = state(c[y], kx);
+          const bool to_y = sx == S_EMIT || (sx == S_HELD && sy == S_EMIT);
+          const bool to_x = sy == S_EMIT || (sy == S_HELD && sx == S_EMIT);
+          double nx = __dmul_rn(c[x], d.cs);
+          if (to_x) nx = __dadd_rn(nx, by);
+          double ny = __dmul_rn(c[y], d.cs);
+          if (to_y) ny = __dadd_rn(ny, bx);
+          c[x] = nx;
+          c[y] = ny;
+        } else {
+          const int l = p[x] ? x : y, o = p[x] ? y : x;
+          const u64* kl = p[x] ? kx : ky;
+          const u64* ko = p[x] ? ky : kx;
+          const double b = __dmul_rn(__dmul_rn(c[l], d.sn), neg_im(Ops::template product_exp<W>(d.g, kl), d.g.sign));
+          const int sl = state(c[l], ko);
+          c[l] = __dmul_rn(c[l], d.cs);
+          if (sl == S_EMIT) {
+            p[o] = true;
+            c[o] = b;
+            born[o] = s;
+          }
+        }
+      };
+      if (a1) {
+        step(d1, 0, 1, 1);
+        if (a2) step(d1, 2, 3, 1);
+      }
+      if (a2) {
+        step(d2, 0, 2, 2);
+        if (a1) step(d2, 1, 3, 2);
+      }
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+        if (j[m] >= 0) coeffs[j[m]] = c[m];
+#pragma unroll
+      for (int m = 1; m < 4; ++m) {
+        if (!born[m]) continue;
+        emit |= 1u << (m - 1);
+        bval[m - 1] = c[m];
+        if (born[m] == 1) {
+          ++n_born1;
+          if (a2) ++n_anti2;  // a row the first rotation creates here anticommutes with the second
+        }
+      }
+    }
+    unsigned masks[3];
+    tile_scan<3>(emit, masks, sm, a.status, t, ntiles, N, epoch, st, n_out);
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (!((emit >> k) & 1u)) continue;
+      const u64 row = N + sm.excl + sm.cnt[k * NWARPS + warp] + __popc(masks[k] & lt);
+      if (row >= a.cap) {
+        atomicOr(&st->error, ERR_CAPACITY);
+        continue;
+      }
+      u64 q[W];
+      member(k + 1, q);
+      store_key<W>(keys, row, q);
+      coeffs[row] = bval[k];
+      insert<W>(q, row, a.table, a.table_mask, &st->error);
+    }
+    __syncthreads();  // sm is reused by the next tile
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n_anti1 += __shfl_xor_sync(FULL, n_anti1, o);
+    n_anti2 += __shfl_xor_sync(FULL, n_anti2, o);
+    n_born1 += __shfl_xor_sync(FULL, n_born1, o);
+  }
+  if (lane == 0) {
+    if (n_anti1 && a.anti) atomicAdd(a.anti + op, (u64)n_anti1);
+    if (n_anti2 && a.anti) atomicAdd(a.anti + op + 1, (u64)n_anti2);
+    if (n_born1) atomicAdd(a.tickets + op, n_born1);  // rows after the first rotation: N + this
+  }
 }
 
 // A rotation with |sin| < 1e-9 only scales the anticommuting rows by cos
@@ -658,13 +826,12 @@ __device__ __noinline__ void noise_scale_op(const SweepArgs& a, const double* fa
 template <int W, int ALG>
 __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* factors, u32 op, u64 N,
                                                  const u64* keys, const double* coeffs, u64* keys_out,
-                                                 double* coeffs_out, TileSmem& sm, const Grp grp) {
+                                                 double* coeffs_out, TileSmem& sm, const Grp grp, u64* n_out) {
   using Ops = typename Alg<ALG>::T;
   constexpr int IT = 1;
   constexpr int TL = BLOCK * IT;
   SweepState* st = a.st;
   const u32 ntiles = (u32)((N + TL - 1) / TL);
-  u64* n_out = &st->n[(op + 1) & 1];
   if (ntiles == 0) {
     if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
     return;
@@ -722,48 +889,71 @@ template <int W, int ALG>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   __shared__ TileSmem sm;
   __shared__ GateDesc<W> sgate[2];  // op k's generator in slot k & 1
+  __shared__ GateDesc<W> sgate2;    // the second generator of a fused op
   __shared__ OpDesc sod[2];
   __shared__ OpShared os;
   SweepState* st = a.st;
   u32 gen = *(volatile u32*)&st->bar_gen;
   int cur = (int)a.cur0;
   u32 op = a.op_begin;
+  // The live count entering the next op is in n[par]; each op writes
+  // n[par ^ 1].  (Not n[op & 1]: a fused op is two ops.)
+  u32 par = op & 1u;
   auto fetch_op = [&](u32 k) {  // thread 0
     if (k >= a.op_end) return;
     const OpDesc d = a.ops[k];
     sod[k & 1] = d;
-    if (d.kind == OP_GATE || d.kind == OP_PHASE) sgate[k & 1] = reinterpret_cast<const GateDesc<W>*>(a.gates)[d.idx];
+    const GateDesc<W>* gd = reinterpret_cast<const GateDesc<W>*>(a.gates);
+    if (d.kind == OP_GATE || d.kind == OP_PHASE || d.kind == OP_GATE2) sgate[k & 1] = gd[d.idx];
+    if (d.kind == OP_GATE2) sgate2 = gd[d.idx + 1];
   };
   if (threadIdx.x == 0) {
     fetch_op(op);
-    os.n = ld_volatile(&st->n[op & 1]);
+    os.n = ld_volatile(&st->n[par]);
   }
   __syncthreads();
-  for (; op < a.op_end; ++op) {
+  while (op < a.op_end) {
     const OpDesc od = sod[op & 1];
     const u64 N = os.n;
     u64* keys = a.keys[cur];
     double* coeffs = a.coeffs[cur];
-    if (od.kind == OP_GATE || od.kind == OP_PHASE) {
-      if (od.kind == OP_GATE && 2 * N > a.cap) {  // uniform: every block reads the same N
+    u64* n_out = &st->n[par ^ 1u];
+    const u32 nops = od.kind == OP_GATE2 ? 2u : 1u;
+    bool split = false;  // a fused op that ran its rotations one after the other
+    if (od.kind == OP_GATE || od.kind == OP_PHASE || od.kind == OP_GATE2) {
+      // uniform: every block reads the same N
+      if ((od.kind == OP_GATE && 2 * N > a.cap) || (od.kind == OP_GATE2 && 4 * N > a.cap)) {
         if (grp.bid == 0 && threadIdx.x == 0) st->halt = op;
         break;
       }
       if (od.kind == OP_GATE) {
-        gate_op<W, ALG>(a, sgate[op & 1], op, N, keys, coeffs, sm, grp);
+        gate_op<W, ALG>(a, sgate[op & 1], op, N, keys, coeffs, sm, grp, n_out);
+      } else if (od.kind == OP_GATE2) {
+        if (N == 0) {
+          if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
+        } else if (N <= (u64)grp.nblk * BLOCK) {
+          gate2_tiles<W, ALG>(a, sgate[op & 1], sgate2, op, N, keys, coeffs, sm, grp, n_out);
+        } else {  // many rows: the two rotations one after the other (op + 1 is the second's slot)
+          split = true;
+          gate_op<W, ALG>(a, sgate[op & 1], op, N, keys, coeffs, sm, grp, &st->n_mid);
+          grid_barrier(st, gen, grp);
+          const u64 N1 = ld_volatile(&st->n_mid);
+          if (grp.bid == 0 && threadIdx.x == 0) a.hist[op] = N1;
+          gate_op<W, ALG>(a, sgate2, op + 1, N1, keys, coeffs, sm, grp, n_out);
+        }
       } else {
         phase_op<W, ALG>(a, sgate[op & 1], op, N, keys, coeffs, grp);
-        if (grp.bid == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
+        if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, N);
       }
     } else if (od.kind == OP_NOISE_SCALE) {
       noise_scale_op<W, ALG>(a, a.tables + (u64)od.idx * a.table_len, N, keys, coeffs, grp);
-      if (grp.bid == 0 && threadIdx.x == 0) st_volatile(&st->n[(op + 1) & 1], N);
+      if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, N);
     } else {
       for (u64 i = (u64)grp.bid * BLOCK + threadIdx.x; i <= a.table_mask; i += (u64)grp.nblk * BLOCK)
         a.table[i] = EMPTY_SLOT;
       grid_barrier(st, gen, grp);
       noise_compact_op<W, ALG>(a, a.tables + (u64)od.idx * a.table_len, op, N, keys, coeffs, a.keys[cur ^ 1],
-                               a.coeffs[cur ^ 1], sm, grp);
+                               a.coeffs[cur ^ 1], sm, grp, n_out);
       cur ^= 1;
     }
     // In a batch, once enough of the grid sits idle every instance stops at
@@ -773,29 +963,33 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     // the same branch (a block reading late sees a later op and goes on).
     if (a.idle_blocks && grp.bid == 0 && threadIdx.x == 0 && *(volatile u32*)a.idle_blocks >= a.yield_at)
       *(volatile u32*)&st->yield_after = op + 1;
-    op_barrier(st, gen, grp, &st->n[(op + 1) & 1], os, [&] { fetch_op(op + 1); });
+    op_barrier(st, gen, grp, n_out, nops == 2 ? a.tickets + op : nullptr, os, [&] { fetch_op(op + nops); });
+    par ^= 1u;
     if (os.err) {
-      ++op;
+      op += nops;
       break;
     }
     if (grp.bid == 0 && threadIdx.x == 0) {
       const u64 n_new = os.n;
-      a.hist[op] = n_new;
+      a.hist[op + nops - 1] = n_new;
+      if (nops == 2 && !split) a.hist[op] = N + os.extra;
       if (n_new > st->peak) st->peak = n_new;
       if (a.stamps) {
         u64 t;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
         a.stamps[op] = t;
+        if (nops == 2) a.stamps[op + 1] = t;
       }
     }
-    if (a.idle_blocks && os.yield_after == op + 1) {
-      ++op;
-      break;
-    }
+    const bool stop = a.idle_blocks && os.yield_after == op + 1;
+    op += nops;
+    if (stop) break;
   }
   if (grp.bid == 0 && threadIdx.x == 0) {
     st->cur = (u32)cur;
     st->end_op = op;
+    // The host reads the live count at n[end_op & 1].
+    if ((op & 1u) != par) st->n[op & 1u] = ld_volatile(&st->n[par]);
     if (a.idle_blocks) atomicAdd(a.idle_blocks, grp.nblk);
   }
 }

@@ -13,6 +13,8 @@ enum OpKind : u32 {
   OP_PHASE = 1,          // |sin| < eps: scale the anticommuting rows by cos
   OP_NOISE_SCALE = 2,    // damp every row by its weight's factor
   OP_NOISE_COMPACT = 3,  // damp, then reclaim: filter + compact + re-insert
+  OP_GATE2 = 4,          // this rotation and the next (whose generators commute) in one pass
+  OP_GATE2_TAIL = 5,     // the second rotation of an OP_GATE2: run by it, skipped by the sweep
 };
 
 struct OpDesc {
@@ -30,6 +32,7 @@ struct GateDesc {
 struct SweepState {
   u64 n[2];       // live rows: op k reads n[k & 1], writes n[(k + 1) & 1]
   u64 peak;       // largest live count the sweeps have seen
+  u64 n_mid;      // live rows between the two rotations of a fused op run one after the other
   u32 halt;       // op at which a sweep stopped for capacity, or NOT_HALTED
   u32 error;      // ERR_* bits
   u32 cur;        // row buffer holding the live rows when the sweep ended
