@@ -180,8 +180,10 @@ typedef struct pq_batch_tuning {
  * GPU together and no instance pays a launch per gate.  The reference runs
  * such sweeps as one expectation_value call after another
  * (ZeroNoiseExtrapolator.run / ZeroCutoffExtrapolator.run,
- * propaq/extrapolators/zne.py:63-108, zce.py:88-137); each instance's result
- * is bit-identical to pq_run's on the same arguments.
+ * propaq/extrapolators/zne.py:63-108, zce.py:88-137); each instance gives
+ * pq_run's terms, coefficients and live counts on the same arguments (new rows
+ * may be appended in another order, so the expectation sum agrees to its last
+ * bits).
  *
  * Keys up to 2x narrower than the widest instance run at half its width;
  * narrower ones are widened with zero words (results are unchanged).

@@ -48,6 +48,9 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr long LOOKBACK_SPIN_LIMIT = 1L << 22;  // ~0.3 s with the backoff below
 constexpr long BARRIER_SPIN_LIMIT = 1L << 25;   // ~2 s with the backoff below
 constexpr u32 BAR_GROUPS = SweepState::BAR_GROUPS;
+// A fused op runs both rotations in one pass while each block has at most
+// this many tiles of rows; above, one after the other.
+constexpr u32 GATE2_TILES_PER_BLOCK = 4;
 
 enum : int { S_EMIT = 0, S_HELD = 1, S_DROP = 2 };
 
@@ -904,7 +907,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     const OpDesc d = a.ops[k];
     sod[k & 1] = d;
     const GateDesc<W>* gd = reinterpret_cast<const GateDesc<W>*>(a.gates);
-    if (d.kind == OP_GATE || d.kind == OP_PHASE || d.kind == OP_GATE2) sgate[k & 1] = gd[d.idx];
+    if (d.kind != OP_NOISE_SCALE && d.kind != OP_NOISE_COMPACT) sgate[k & 1] = gd[d.idx];
     if (d.kind == OP_GATE2) sgate2 = gd[d.idx + 1];
   };
   if (threadIdx.x == 0) {
@@ -913,7 +916,10 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   }
   __syncthreads();
   while (op < a.op_end) {
-    const OpDesc od = sod[op & 1];
+    OpDesc od = sod[op & 1];
+    // A launch that resumes between the two rotations of a fused op (after a
+    // capacity stop) runs the second as a plain rotation.
+    if (od.kind == OP_GATE2_TAIL) od.kind = OP_GATE;
     const u64 N = os.n;
     u64* keys = a.keys[cur];
     double* coeffs = a.coeffs[cur];
@@ -921,8 +927,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     const u32 nops = od.kind == OP_GATE2 ? 2u : 1u;
     bool split = false;  // a fused op that ran its rotations one after the other
     if (od.kind == OP_GATE || od.kind == OP_PHASE || od.kind == OP_GATE2) {
-      // uniform: every block reads the same N
-      if ((od.kind == OP_GATE && 2 * N > a.cap) || (od.kind == OP_GATE2 && 4 * N > a.cap)) {
+      if (2 * N > a.cap) {  // uniform: every block reads the same N
         if (grp.bid == 0 && threadIdx.x == 0) st->halt = op;
         break;
       }
@@ -931,7 +936,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
       } else if (od.kind == OP_GATE2) {
         if (N == 0) {
           if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
-        } else if (N <= (u64)grp.nblk * BLOCK) {
+        } else if (N <= (u64)grp.nblk * BLOCK * GATE2_TILES_PER_BLOCK && 4 * N <= a.cap) {
           gate2_tiles<W, ALG>(a, sgate[op & 1], sgate2, op, N, keys, coeffs, sm, grp, n_out);
         } else {  // many rows: the two rotations one after the other (op + 1 is the second's slot)
           split = true;
@@ -939,6 +944,20 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
           grid_barrier(st, gen, grp);
           const u64 N1 = ld_volatile(&st->n_mid);
           if (grp.bid == 0 && threadIdx.x == 0) a.hist[op] = N1;
+          if (2 * N1 > a.cap) {  // stop before the second rotation
+            if (grp.bid == 0 && threadIdx.x == 0) {
+              st->n[par] = N1;  // read as the next op's count (nobody reads n[par] during this op)
+              st->halt = op + 1;
+              if (N1 > st->peak) st->peak = N1;
+              if (a.stamps) {
+                u64 t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                a.stamps[op] = t;
+              }
+            }
+            ++op;
+            break;
+          }
           gate_op<W, ALG>(a, sgate2, op + 1, N1, keys, coeffs, sm, grp, n_out);
         }
       } else {

@@ -94,12 +94,15 @@ def test_checkpoint_segments_do_not_change_the_gradient(gpu_engine):
 
 
 def test_forward_part_equals_plain_run(gpu_engine):
+    # The gradient's forward pass runs every rotation on its own while a plain
+    # run fuses commuting pairs; the terms are the same, appended in another
+    # order, so only the expectation sum's last bits may differ.
     wl = workloads.kicked_ising(5, 6, 4)
     p = from_workload(wl)
     cfg, keep = make_cfg(p, want_terms=False)
     plain, nt_plain = gpu_engine.run(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag)
     res, nt, g = gpu_grad(gpu_engine, p, 2)
-    assert res.expectation_value == plain.expectation_value
+    assert abs(res.expectation_value - plain.expectation_value) <= 1e-12 * max(1.0, abs(plain.expectation_value))
     assert np.array_equal(nt, nt_plain)
     assert np.isfinite(g[np.abs(np.cos(p.angles)) >= 1e-9]).all()
 

@@ -269,6 +269,21 @@ def test_capacity_growth_and_engine_reuse(gpu_engine, oracle):
     assert a.expectation == b.expectation
 
 
+def test_capacity_stops_inside_fused_rotations(oracle):
+    # A fresh engine starts at 64 Ki rows, so this run stops for capacity many
+    # times, some of them between the two rotations of a fused pair (the second
+    # then runs alone when the sweep resumes).
+    from propaq_b200 import _native
+
+    eng = _native.Engine(0)
+    p = from_workload(workloads.kicked_ising(4, 4, 6))
+    g = run_gpu(eng, p)
+    o = run_oracle(oracle, p)
+    assert g.res.sweep_launches > 3
+    assert np.array_equal(g.n_terms, o.n_terms)
+    assert_terms_equal(g.keys, g.coeffs, o.keys, o.coeffs)
+
+
 def test_width_errors(gpu_engine):
     big = PauliTermSum({PauliString(0, 1, 2049): 1.0})
     with pytest.raises(ValueError, match="exceeds the engine's maximum of 2048"):
