@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "majorana", "majorana_small", "tfim", "batch", "adjoint"])
+    ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "kicked_ising_small", "majorana", "majorana_small", "tfim", "batch", "adjoint"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="sweep blocks per SM (0 = as many as fit)")
@@ -76,6 +76,10 @@ def make_workload(name):
         wl = workloads.kicked_ising()
         desc = ("kicked Ising 10x10 open lattice, 20 steps, RZZ(-pi/2) x 180 edges + RX(0.6) x 100 per step, "
                 "Z(centre), p=1e-3 depolarising as (1-p)^w, w<=10, |c|>=1e-5")
+    elif name == "kicked_ising_small":
+        wl = workloads.kicked_ising(steps=8)
+        desc = ("kicked Ising 10x10 open lattice, 8 steps, RZZ(-pi/2) + RX(0.6), Z(centre), p=1e-3, w<=10, "
+                "|c|>=1e-5 (profiling case)")
     elif name == "majorana_small":
         wl = workloads.majorana_givens(n_sites=24, reps=3)
         desc = ("Majorana 24 sites / 48 modes, 3 reps of brick-wall Givens + number-number phases |p-q|<=3, "
