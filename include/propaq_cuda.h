@@ -227,6 +227,16 @@ int pq_plugin_load_noise(const char* path, const char* config_json, pq_plugin** 
 int pq_plugin_load_truncator(const char* path, const char* config_json, pq_plugin** out,
                              char* err, size_t err_len);
 void pq_plugin_free(pq_plugin* plugin);
+/* A noise model given as a function of the caller's, with the plugin ABI's
+ * factor signature; `depends` as propaq_noise_depends (bit 0 KEY, bit 1
+ * LAYER).  It replaces the Python damping_factor_term hook path
+ * (crates/core/src/engine/noise_resolver.rs:28-37, ResolvedNoise::PythonTerm;
+ * crates/pauli/src/engine.rs:142-158): the host calls it for every live term
+ * at each noise op.  Free with pq_plugin_free. */
+typedef double (*pq_noise_factor_fn)(void* ctx, uint32_t basis_kind, const uint64_t* words, size_t n_words,
+                                     uint32_t n_units, uint32_t weight, uint32_t layer_index,
+                                     uint32_t n_layers);
+int pq_plugin_from_callback(pq_noise_factor_fn fn, void* ctx, uint32_t depends, pq_plugin** out);
 uint32_t pq_plugin_depends(const pq_plugin* plugin);
 /* NativeNoiseModel.factor_term (native_noise.rs:316-333). */
 double pq_plugin_noise_factor(const pq_plugin* plugin, uint32_t basis_kind, const uint64_t* words,

@@ -111,6 +111,10 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_uint32), ("split", ctypes.c_uint32), ("rebalance_pct", ctypes.c_uint32)]
 
 
+NOISE_FACTOR_FN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64),
+                                   ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                   ctypes.c_uint32)
+
 _SIGNATURES = {
     "pq_words_for_units": (_U32, [_U32]),
     "pq_engine_create": (ctypes.c_int, [ctypes.POINTER(_V), ctypes.c_int]),
@@ -128,6 +132,7 @@ _SIGNATURES = {
     "pq_plugin_load_truncator": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_V),
                                                 ctypes.c_char_p, _Z]),
     "pq_plugin_free": (None, [_V]),
+    "pq_plugin_from_callback": (ctypes.c_int, [NOISE_FACTOR_FN, _V, _U32, ctypes.POINTER(_V)]),
     "pq_plugin_depends": (_U32, [_V]),
     "pq_plugin_noise_factor": (ctypes.c_double, [_V, _U32, _V, _Z, _U32, _U32, _U32, _U32]),
     "pq_plugin_truncator_keep": (ctypes.c_int, [_V, _U32, _V, _Z, _U32, _U32, ctypes.c_double, _U32, _U32]),
@@ -330,6 +335,50 @@ class Plugin:
         w = np.ascontiguousarray(list(words), dtype=np.uint64)
         return bool(lib().pq_plugin_truncator_keep(self._h, basis_kind, _ptr(w) if len(w) else None, len(w),
                                                    n_units, weight, coeff_magnitude, layer_index, n_layers))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.pq_plugin_free(h)
+            self._h = None
+
+
+class CallbackNoise:
+    """A Python function of (basis_kind, words, n_units, weight, layer_index,
+    n_layers) as a noise plugin handle (pq_plugin_from_callback).  An
+    exception inside the function is kept, the factor of that call is NaN, and
+    `raise_pending()` re-raises it after the run."""
+
+    def __init__(self, fn, depends: int):
+        self._fn = fn
+        self.error = None
+
+        def trampoline(ctx, basis_kind, words, n_words, n_units, weight, layer, n_layers):
+            if self.error is not None:
+                return float("nan")
+            try:
+                w = [int(words[i]) for i in range(n_words)] if words else []
+                return float(fn(basis_kind, w, n_units, weight, layer, n_layers))
+            except BaseException as exc:  # noqa: BLE001 -- re-raised by raise_pending
+                self.error = exc
+                return float("nan")
+
+        self._cb = NOISE_FACTOR_FN(trampoline)
+        handle = ctypes.c_void_p()
+        rc = lib().pq_plugin_from_callback(self._cb, None, depends, ctypes.byref(handle))
+        if rc != PQ_OK:
+            raise_for(rc, "could not wrap the noise callback")
+        self._h = handle
+        self.depends = depends
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def raise_pending(self):
+        if self.error is not None:
+            err, self.error = self.error, None
+            raise err
 
     def __del__(self):
         h = getattr(self, "_h", None)

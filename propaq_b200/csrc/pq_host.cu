@@ -257,6 +257,11 @@ struct Plugin {
 };
 typedef double (*NoiseFactorFn)(void*, u32, const u64*, size_t, u32, u32, u32, u32);
 typedef int32_t (*KeepFn)(void*, u32, const u64*, size_t, u32, u32, double, u32, u32);
+// The batch forms (native_noise.rs:142-188, native_truncator.rs:158-200): 0 = done.
+typedef int32_t (*NoiseBatchFn)(void*, u32, const u64*, size_t, u32, const u32*, u32, u32, double*, size_t);
+typedef int32_t (*KeepBatchFn)(void*, u32, const u64*, size_t, u32, const u32*, const double*, u32, u32, uint8_t*,
+                               size_t);
+constexpr size_t KERNEL_BATCH = 1024;  // term_kernel.rs:10
 
 void set_err(char* err, size_t n, const std::string& m) {
   if (err && n) snprintf(err, n, "%s", m.c_str());
@@ -361,6 +366,10 @@ struct Slot {
   u64* frame_img = nullptr;  // readout tableau of the last run, when not the identity
   int* frame_sgn = nullptr;
   size_t frame_cap = 0;
+  unsigned char* host_state = nullptr;  // decisions made on the host for one op (see SweepArgs)
+  double* host_factor = nullptr;
+  unsigned char* host_keep = nullptr;
+  size_t host_cap = 0;
   int out_words = 0;  // width of out_keys (the caller's width)
   std::vector<u64> out_keys;
   std::vector<double> out_coeffs;
@@ -389,8 +398,13 @@ struct Slot {
   void free_all() {
     free_rows();
     free_ops();
-    for (void* p : {(void*)d_gates, (void*)d_tables, (void*)partials, (void*)frame_img, (void*)frame_sgn})
+    for (void* p : {(void*)d_gates, (void*)d_tables, (void*)partials, (void*)frame_img, (void*)frame_sgn,
+                    (void*)host_state, (void*)host_factor, (void*)host_keep})
       if (p) cudaFree(p);
+    host_state = nullptr;
+    host_factor = nullptr;
+    host_keep = nullptr;
+    host_cap = 0;
     d_gates = nullptr;
     d_tables = nullptr;
     partials = nullptr;
@@ -603,6 +617,14 @@ struct Plan {
   size_t tlen = 0;
   std::vector<double> tables;
   bool layered = false, have_noise = false;
+  // Plugins the host consults during the run (noise_resolver.rs:28-37,
+  // termsum.rs:113-168): a truncator decides every branch and reclaim; a
+  // key-reading noise model gives every row its own factor.  Either one
+  // reading keys turns Clifford deferral off (engine.rs:101-103).
+  const Plugin* term = nullptr;
+  const Plugin* keynoise = nullptr;
+  bool host_ops = false;
+  bool defer = true;
   std::vector<u64> hk;
   std::vector<double> hc;
   u64 n0 = 0;
@@ -656,15 +678,16 @@ int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
     P.layered = true;
   } else if (cfg->noise_kind == PQ_NOISE_PLUGIN) {
     if (!np) return E->fail(PQ_ERR_INVALID, "noise plugin missing");
-    if (np->depends & 1)
-      return E->fail(PQ_ERR_UNSUPPORTED, "key-reading noise plugins are not run by the CUDA engine yet");
     P.tlen = (size_t)P.n_units + 1;
+    if (np->depends & 1) P.keynoise = np;
     auto f = (NoiseFactorFn)np->fn;
     auto tab = [&](u32 layer, u32 total) {
       for (u32 w = 0; w < P.n_units + 1; ++w)
         P.tables.push_back(f(np->ctx, ALG, nullptr, 0, P.n_units, w, layer, total));
     };
-    if (np->depends & 2) {
+    if (P.keynoise) {
+      // per term, on the host at each noise op
+    } else if (np->depends & 2) {
       P.layered = true;
       for (size_t l = 0; l < in.n_layers; ++l) tab((u32)l, (u32)in.n_layers);
     } else {
@@ -673,8 +696,11 @@ int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
   } else if (cfg->noise_kind != PQ_NOISE_NONE) {
     return E->fail(PQ_ERR_INVALID, "unknown noise kind");
   }
-  if (cfg->truncator)
-    return E->fail(PQ_ERR_UNSUPPORTED, "native truncator plugins are not run by the CUDA engine yet");
+  P.term = reinterpret_cast<const Plugin*>(cfg->truncator);
+  if (P.term && P.term->noise) return E->fail(PQ_ERR_INVALID, "the truncator handle is a noise plugin");
+  if (P.keynoise && !P.keynoise->noise) return E->fail(PQ_ERR_INVALID, "the noise handle is a truncator plugin");
+  P.host_ops = P.term || P.keynoise;
+  P.defer = !(P.keynoise || (P.term && (P.term->depends & 1)));
   struct H {
     size_t operator()(const std::vector<u64>& v) const {
       u64 h = 0x9e3779b97f4a7c15ULL;
@@ -690,8 +716,15 @@ int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
   for (size_t i = 0; i < in.n_obs; ++i) {
     P.widen(in.obs_words, i, k.data());
     const double c = in.obs_coeffs[i];
-    if (P.has_w && host_weight(ALG, W, k.data(), P.n_units) > P.wcut) continue;
-    if (P.has_c && !(std::fabs(c) >= P.ccut)) continue;
+    if (P.term) {  // admits_initial with a term kernel: its keep alone (termsum.rs:113-160)
+      const bool kd = P.term->depends & 1;
+      if (!((KeepFn)P.term->fn)(P.term->ctx, ALG, kd ? k.data() : nullptr, kd ? (size_t)W : 0, P.n_units,
+                                host_weight(ALG, W, k.data(), P.n_units), std::fabs(c), 0, 0))
+        continue;
+    } else {
+      if (P.has_w && host_weight(ALG, W, k.data(), P.n_units) > P.wcut) continue;
+      if (P.has_c && !(std::fabs(c) >= P.ccut)) continue;
+    }
     auto it = pos.find(k);
     if (it != pos.end()) {
       P.hc[it->second] += c;
@@ -766,7 +799,7 @@ int build_ops(Plan& P, NeedN need_n) {
     P.layer_op.push_back(P.ops.size());
     if (P.have_noise) {
       pq::OpDesc od;
-      od.kind = (P.has_w || P.has_c) ? pq::OP_NOISE_COMPACT : pq::OP_NOISE_SCALE;  // partitioned_termsum.rs:585-587
+      od.kind = (P.has_w || P.has_c || P.term) ? pq::OP_NOISE_COMPACT : pq::OP_NOISE_SCALE;  // partitioned_termsum.rs:585-587
       od.idx = P.layered ? (u32)l : 0u;
       P.ops.push_back(od);
       P.last_op = (long)P.ops.size() - 1;
@@ -774,7 +807,7 @@ int build_ops(Plan& P, NeedN need_n) {
     for (u32 gi = in.layer_off[l]; gi < in.layer_off[l + 1]; ++gi) {
       P.widen(in.gate_words, gi, g.data());
       const double ang = in.angles[gi];
-      if (std::fabs(std::cos(ang)) < EPS_CLASSIFY) {  // Clifford: defer into the frame when allowed
+      if (P.defer && std::fabs(std::cos(ang)) < EPS_CLASSIFY) {  // Clifford: defer into the frame when allowed
         bool eff_w = P.has_w;
         const bool cw = Tableau::rotation_changes_weight(ALG, W, P.n_units, g.data());
         if (P.has_w && cw && P.has_floor) {  // the effective cutoff depends on the live count here
@@ -820,7 +853,7 @@ int build_ops(Plan& P, NeedN need_n) {
 // live count between the two rotations.  The reverse sweep of the adjoint
 // needs each rotation's own record, so its runs do not fuse.
 void fuse_pairs(Plan& P) {
-  if (P.has_floor) return;
+  if (P.has_floor || P.host_ops) return;
   const size_t gw = gdesc_words(P.W);
   for (size_t i = 0; i + 1 < P.ops.size(); ++i) {
     if (P.ops[i].kind != pq::OP_GATE || P.ops[i + 1].kind != pq::OP_GATE) continue;
@@ -858,8 +891,16 @@ struct Recording {
   u64* key_off = nullptr;
 };
 
+// Per-row decisions made on the host for one op (device pointers, or null).
+struct HostOps {
+  const unsigned char* state = nullptr;
+  const double* factor = nullptr;
+  const unsigned char* keep = nullptr;
+};
+
 pq::SweepArgs sweep_args(Slot& S, const Plan& P, pq::SweepState* st, u32 blk_begin, u32 blk_count,
-                         size_t op_limit = (size_t)-1, const Recording* rec = nullptr) {
+                         size_t op_limit = (size_t)-1, const Recording* rec = nullptr,
+                         const HostOps* host = nullptr) {
   pq::SweepArgs a{};
   a.ops = S.d_ops;
   a.gates = S.d_gates;
@@ -869,6 +910,11 @@ pq::SweepArgs sweep_args(Slot& S, const Plan& P, pq::SweepState* st, u32 blk_beg
   a.n_words = (u32)P.W;
   a.op_begin = (u32)P.done;
   a.op_end = (u32)std::min(op_limit, P.ops.size());
+  if (host) {
+    a.host_state = host->state;
+    a.host_factor = host->factor;
+    a.host_keep = host->keep;
+  }
   if (rec) {
     a.rec_idx = rec->idx;
     a.rec_coef = rec->coef;
@@ -937,8 +983,8 @@ int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
 
 // Runs every built op of one plan on the whole grid, relaunching after
 // capacity growth.
-int execute_single(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size_t op_limit = (size_t)-1,
-                   const Recording* rec = nullptr) {
+int execute_launches(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size_t op_limit,
+                     const Recording* rec, const HostOps* host) {
   cudaError_t e;
   upload_ops(E, S, P);
   const size_t end = std::min(op_limit, P.ops.size());
@@ -946,7 +992,7 @@ int execute_single(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size_t
     E->h_states[0] = fresh_state(P);
     cudaMemcpyAsync(E->d_states, E->h_states, sizeof(pq::SweepState), cudaMemcpyHostToDevice, E->stream);
     cudaMemsetAsync(S.tickets + P.done, 0, (end - P.done) * 4, E->stream);
-    const pq::SweepArgs a = sweep_args(S, P, E->d_states, 0, (u32)grid, end, rec);
+    const pq::SweepArgs a = sweep_args(S, P, E->d_states, 0, (u32)grid, end, rec, host);
     if (!*began) {  // device time starts at the first sweep
       cudaEventRecord(E->ev_begin, E->stream);
       *began = true;
@@ -965,6 +1011,155 @@ int execute_single(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size_t
     cudaEventElapsedTime(&ms, E->ev_l0, E->ev_l1);
     P.sweep_ms += ms;
     if (int rc = absorb_state(E, S, P, E->h_states[0])) return rc;
+  }
+  return PQ_OK;
+}
+
+// True if op k needs decisions from a plugin on the host: every rotation when
+// a truncator is set (its keep decides each branch), every noise op when the
+// noise model reads keys or a truncator decides the reclaim.
+bool needs_host(const Plan& P, size_t k) {
+  const u32 kind = P.ops[k].kind;
+  if (kind == pq::OP_GATE) return P.term != nullptr;
+  if (kind == pq::OP_NOISE_SCALE || kind == pq::OP_NOISE_COMPACT) return P.keynoise || P.term;
+  return false;
+}
+
+u32 layer_of(const Plan& P, size_t k) {
+  const auto it = std::upper_bound(P.layer_op.begin(), P.layer_op.end(), k);
+  return (u32)(it - P.layer_op.begin()) - 1;
+}
+
+// Reads the live rows back and asks the plugins for op k's decisions, exactly
+// where the reference asks them: a truncator's scalar keep for every branch
+// (termsum.rs:701-751, with the branch's coefficient and child key), a
+// key-reading noise model's factor for every row (factor_batch in chunks of
+// 1024 when the plugin has it, termsum.rs:340-371), and the truncator's
+// keep_batch on the damped rows for the reclaim (termsum.rs:387-447).  A
+// rotation under the TermBudget floor runs with no truncation at all.
+int host_decide(pq_engine* E, Slot& S, Plan& P, size_t k, HostOps* ho) {
+  *ho = HostOps{};
+  const int W = P.W, ALG = P.alg;
+  const u64 N = P.n_live;
+  const u32 kind = P.ops[k].kind;
+  if (kind == pq::OP_GATE && P.has_floor && N < P.floor_terms) return PQ_OK;
+  if (N == 0) return PQ_OK;
+  cudaError_t e;
+  if (S.host_cap < N) {
+    for (void* p : {(void*)S.host_state, (void*)S.host_factor, (void*)S.host_keep})
+      if (p) cudaFree(p);
+    S.host_state = nullptr;
+    S.host_factor = nullptr;
+    S.host_keep = nullptr;
+    S.host_cap = 0;
+    const size_t cap = std::max<size_t>(N, S.cap);
+    if ((e = cudaMalloc(&S.host_state, cap)) != cudaSuccess || (e = cudaMalloc(&S.host_factor, cap * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&S.host_keep, cap)) != cudaSuccess)
+      return E->cuda_fail(e, "host decision buffers");
+    S.host_cap = cap;
+  }
+  std::vector<u64> keys(N * W);
+  std::vector<double> co(N);
+  cudaMemcpyAsync(keys.data(), S.keys[S.cur], N * W * 8, cudaMemcpyDeviceToHost, E->stream);
+  cudaMemcpyAsync(co.data(), S.coeffs[S.cur], N * 8, cudaMemcpyDeviceToHost, E->stream);
+  if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "reading rows back");
+  const u32 layer = layer_of(P, k), n_layers = (u32)P.in->n_layers;
+  if (kind == pq::OP_GATE) {
+    const Plugin* t = P.term;
+    const bool kd = t->depends & 1;
+    std::vector<u64> gen(W), child(W);
+    double sign = 1.0, sn = 0.0;
+    with_words(W, [&](auto w) {
+      constexpr int WW = decltype(w)::value;
+      pq::GateDesc<WW> gd;
+      std::memcpy(&gd, &P.gdesc[P.ops[k].idx * gdesc_words(W)], sizeof gd);
+      for (int i = 0; i < WW; ++i) gen[i] = gd.g.gen[i];
+      sign = gd.g.sign;
+      sn = gd.sn;
+      return 0;
+    });
+    std::vector<unsigned char> st(N, 0);
+    for (u64 r = 0; r < N; ++r) {
+      const u64* kr = &keys[r * W];
+      if (!host_anticommutes(ALG, W, gen.data(), kr)) continue;
+      for (int i = 0; i < W; ++i) child[i] = kr[i] ^ gen[i];
+      const int p = host_product_exp(ALG, W, gen.data(), kr);
+      const double ni = p == 1 ? -sign : (p == 3 ? sign : 0.0);
+      const double b = (co[r] * sn) * ni;
+      const bool keep = ((KeepFn)t->fn)(t->ctx, ALG, kd ? child.data() : nullptr, kd ? (size_t)W : 0, P.n_units,
+                                        host_weight(ALG, W, child.data(), P.n_units), std::fabs(b), layer,
+                                        n_layers) != 0;
+      st[r] = keep ? 0 : 1;  // S_EMIT : S_HELD
+    }
+    cudaMemcpyAsync(S.host_state, st.data(), N, cudaMemcpyHostToDevice, E->stream);
+    ho->state = S.host_state;
+  } else {
+    std::vector<u32> wts(N);
+    for (u64 r = 0; r < N; ++r) wts[r] = host_weight(ALG, W, &keys[r * W], P.n_units);
+    std::vector<double> f(N);
+    if (P.keynoise) {
+      const Plugin* np = P.keynoise;
+      const bool kd = np->depends & 1;
+      for (u64 s0 = 0; s0 < N; s0 += KERNEL_BATCH) {
+        const size_t len = (size_t)std::min<u64>(KERNEL_BATCH, N - s0);
+        bool done = false;
+        if (np->batch_fn)
+          done = ((NoiseBatchFn)np->batch_fn)(np->ctx, ALG, kd ? &keys[s0 * W] : nullptr, kd ? (size_t)W : 0,
+                                              P.n_units, &wts[s0], layer, n_layers, &f[s0], len) == 0;
+        if (!done)
+          for (size_t j = 0; j < len; ++j)
+            f[s0 + j] = ((NoiseFactorFn)np->fn)(np->ctx, ALG, kd ? &keys[(s0 + j) * W] : nullptr,
+                                                kd ? (size_t)W : 0, P.n_units, wts[s0 + j], layer, n_layers);
+      }
+      cudaMemcpyAsync(S.host_factor, f.data(), N * 8, cudaMemcpyHostToDevice, E->stream);
+      ho->factor = S.host_factor;
+    } else {
+      const double* tab = P.tables.data() + (P.layered ? (size_t)P.ops[k].idx * P.tlen : 0);
+      for (u64 r = 0; r < N; ++r) f[r] = tab[std::min<size_t>(wts[r], P.tlen - 1)];
+    }
+    if (P.term && kind == pq::OP_NOISE_COMPACT) {
+      const Plugin* t = P.term;
+      const bool kd = t->depends & 1;
+      std::vector<double> mags(N);
+      for (u64 r = 0; r < N; ++r) mags[r] = std::fabs(co[r] * f[r]);
+      std::vector<unsigned char> keep(N);
+      for (u64 s0 = 0; s0 < N; s0 += KERNEL_BATCH) {
+        const size_t len = (size_t)std::min<u64>(KERNEL_BATCH, N - s0);
+        bool done = false;
+        if (t->batch_fn)
+          done = ((KeepBatchFn)t->batch_fn)(t->ctx, ALG, kd ? &keys[s0 * W] : nullptr, kd ? (size_t)W : 0,
+                                            P.n_units, &wts[s0], &mags[s0], layer, n_layers, &keep[s0], len) == 0;
+        if (done) {
+          for (size_t j = 0; j < len; ++j) keep[s0 + j] = keep[s0 + j] != 0;
+        } else {
+          for (size_t j = 0; j < len; ++j)
+            keep[s0 + j] = ((KeepFn)t->fn)(t->ctx, ALG, kd ? &keys[(s0 + j) * W] : nullptr, kd ? (size_t)W : 0,
+                                           P.n_units, wts[s0 + j], mags[s0 + j], layer, n_layers) != 0;
+        }
+      }
+      cudaMemcpyAsync(S.host_keep, keep.data(), N, cudaMemcpyHostToDevice, E->stream);
+      ho->keep = S.host_keep;
+    }
+  }
+  return PQ_OK;
+}
+
+// Runs ops up to op_limit: whole stretches in one launch, and every op that
+// needs a plugin's decisions on its own, after host_decide.
+int execute_single(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size_t op_limit = (size_t)-1,
+                   const Recording* rec = nullptr) {
+  if (!P.host_ops) return execute_launches(E, S, P, grid, began, op_limit, rec, nullptr);
+  const size_t end = std::min(op_limit, P.ops.size());
+  while (P.done < end) {
+    size_t h = P.done;
+    while (h < end && !needs_host(P, h)) ++h;
+    if (h > P.done) {
+      if (int rc = execute_launches(E, S, P, grid, began, h, rec, nullptr)) return rc;
+      continue;
+    }
+    HostOps ho;
+    if (int rc = host_decide(E, S, P, h, &ho)) return rc;
+    if (int rc = execute_launches(E, S, P, grid, began, h + 1, rec, &ho)) return rc;
   }
   return PQ_OK;
 }
@@ -1189,6 +1384,8 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, double* 
   Slot& S = E->slots[0];
   Plan P;
   if (int rc = prepare(E, P, in, W)) return rc;
+  if (P.host_ops)
+    return E->fail(PQ_ERR_UNSUPPORTED, "the gradient does not run truncator plugins or key-reading noise");
   if (int rc = setup_slot(E, S, P)) return rc;
   const int ALG = P.alg;
   const int grid = with_words(W, [&](auto w) {
@@ -1404,6 +1601,8 @@ int run_batch(pq_engine* E, const std::vector<Inputs>& ins, int WM, const pq_bat
   for (size_t i = 0; i < n; ++i) {
     const int W = std::max(ins[i].in_words, WM > 1 ? WM / 2 : 1);
     if (int rc = prepare(E, plans[i], ins[i], W)) return rc;
+    if (plans[i].host_ops)
+      return E->fail(PQ_ERR_UNSUPPORTED, "a batch does not run truncator plugins or key-reading noise; use pq_run");
     if (int rc = setup_slot(E, E->slots[i], plans[i])) return rc;
     if (int rc = build_ops(plans[i], no_sync)) return rc;
     fuse_pairs(plans[i]);
@@ -1636,6 +1835,18 @@ int pq_plugin_load_truncator(const char* path, const char* cfg, pq_plugin** out,
   return load_plugin(false, path, cfg, out, err, n);
 }
 void pq_plugin_free(pq_plugin* p) { delete reinterpret_cast<Plugin*>(p); }
+
+int pq_plugin_from_callback(pq_noise_factor_fn fn, void* ctx, uint32_t depends, pq_plugin** out) {
+  if (!fn || !out) return PQ_ERR_INVALID;
+  if (depends & ~3u) return PQ_ERR_PLUGIN;
+  auto* p = new Plugin;
+  p->noise = true;
+  p->ctx = ctx;
+  p->depends = depends;
+  p->fn = reinterpret_cast<void*>(fn);
+  *out = reinterpret_cast<pq_plugin*>(p);
+  return PQ_OK;
+}
 uint32_t pq_plugin_depends(const pq_plugin* p) { return reinterpret_cast<const Plugin*>(p)->depends; }
 double pq_plugin_noise_factor(const pq_plugin* pp, uint32_t kind, const uint64_t* words, size_t nw, uint32_t n_units,
                               uint32_t weight, uint32_t layer, uint32_t n_layers) {

@@ -463,7 +463,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
 #pragma unroll
       for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ g.gen[w];
       const double bi = __dmul_rn(__dmul_rn(c[k], sn), neg_im(Ops::template product_exp<W>(g, key[k]), g.sign));
-      const int si = state(c[k], q);
+      const int si = a.host_state ? (int)a.host_state[r] : state(c[k], q);
       if (j[k] < 0) {
         coeffs[r] = __dmul_rn(c[k], cs);
         if (si == S_EMIT) {
@@ -474,7 +474,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
         if (a.rec_idx) record_single(a, op, r, c[k]);
       } else {
         const double bj = __dmul_rn(__dmul_rn(cj[k], sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
-        const int sj = state(cj[k], key[k]);
+        const int sj = a.host_state ? (int)a.host_state[j[k]] : state(cj[k], key[k]);
         const bool to_j = si == S_EMIT || (si == S_HELD && sj == S_EMIT);
         const bool to_i = sj == S_EMIT || (sj == S_HELD && si == S_EMIT);
         double ni = __dmul_rn(c[k], cs);
@@ -559,7 +559,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
       if (j >= 0 && (u64)j < r) continue;  // the lower row of the pair owns it
       const double c = __ldcg(coeffs + r);
       const double bi = __dmul_rn(__dmul_rn(c, sn), neg_im(Ops::template product_exp<W>(g, key), g.sign));
-      const int si = state(c, q);
+      const int si = a.host_state ? (int)a.host_state[r] : state(c, q);
       if (j < 0) {
         coeffs[r] = __dmul_rn(c, cs);
         if (si == S_EMIT) {
@@ -570,7 +570,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
       } else {
         const double cj = __ldcg(coeffs + j);
         const double bj = __dmul_rn(__dmul_rn(cj, sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
-        const int sj = state(cj, key);
+        const int sj = a.host_state ? (int)a.host_state[j] : state(cj, key);
         const bool to_j = si == S_EMIT || (si == S_HELD && sj == S_EMIT);
         const bool to_i = sj == S_EMIT || (sj == S_HELD && si == S_EMIT);
         double ni = __dmul_rn(c, cs);
@@ -819,7 +819,8 @@ __device__ __noinline__ void noise_scale_op(const SweepArgs& a, const double* fa
     u64 key[W];
     load_key<W>(keys, r, key);
     const u32 w = Ops::template weight<W>(key, a.n_units);
-    coeffs[r] = __dmul_rn(__ldcg(coeffs + r), __ldg(factors + (w < last ? w : last)));
+    const double f = a.host_factor ? __ldg(a.host_factor + r) : __ldg(factors + (w < last ? w : last));
+    coeffs[r] = __dmul_rn(__ldcg(coeffs + r), f);
   }
 }
 
@@ -860,10 +861,12 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
       const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
       if (r >= N) continue;
       const u32 w = Ops::template weight<W>(key[k], a.n_units);
-      const double c = __dmul_rn(cv[k], __ldg(factors + (w < last ? w : last)));
+      const double f = a.host_factor ? __ldg(a.host_factor + r) : __ldg(factors + (w < last ? w : last));
+      const double c = __dmul_rn(cv[k], f);
       cv[k] = c;
-      const bool kp = (a.max_weight == NO_WEIGHT_CUT || w <= a.max_weight) &&
-                      (!a.has_min_coeff || fabs(c) >= a.min_coeff);
+      const bool kp = a.host_keep ? a.host_keep[r] != 0
+                                  : (a.max_weight == NO_WEIGHT_CUT || w <= a.max_weight) &&
+                                        (!a.has_min_coeff || fabs(c) >= a.min_coeff);
       keep |= (u32)kp << k;
       if (kp) slot[k] = claim_slot<W>(key[k], a.table, a.table_mask, &st->error);
       if (a.rec_idx) {

@@ -84,6 +84,14 @@ struct SweepArgs {
   u64* rec_keys;
   const u64* rec_off;
   const u64* rec_key_off;
+  // Decisions made on the host for a launch of one op (null: the device's own
+  // rules).  host_state: per input row, the emit state of its sin branch
+  // (S_EMIT 0 / S_HELD 1), from a truncator plugin's keep.  host_factor: per
+  // row, the noise factor (a key-reading noise model).  host_keep: per row,
+  // the reclaim decision (a truncator plugin's keep_batch).
+  const unsigned char* host_state;
+  const double* host_factor;
+  const unsigned char* host_keep;
 };
 
 constexpr u32 REC_NONE = 0xffffffffu;

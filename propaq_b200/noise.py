@@ -79,10 +79,12 @@ def resolve_noise(model, n_units: int):
         table = np.array([math.exp(-d * float(w)) for w in range(n_units + 1)], dtype=np.float64)
         return _native.PQ_NOISE_TABLE, table, None
     if isinstance(model, NativeNoiseModel):
-        if model.depends & 1:
-            raise NotImplementedError("key-reading noise plugins are not run by the CUDA engine yet")
         return _native.PQ_NOISE_PLUGIN, None, model
     if hasattr(model, PYTHON_TERM_HOOK):
-        raise NotImplementedError("key-aware Python noise hooks are not run by the CUDA engine yet")
+        # ResolvedNoise::PythonTerm: called per live term at every noise op, with
+        # the reference's arguments (basis_kind, words, n_units, weight).
+        hook = getattr(model, PYTHON_TERM_HOOK)
+        return _native.PQ_NOISE_PLUGIN, None, _native.CallbackNoise(
+            lambda kind, words, n_units, weight, layer, n_layers: hook(kind, words, n_units, weight), 1)
     table = np.array([float(model.damping_factor(w, 0)) for w in range(n_units + 1)], dtype=np.float64)
     return _native.PQ_NOISE_TABLE, table, None

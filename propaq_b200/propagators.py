@@ -155,7 +155,15 @@ class _Propagator:
     def _run(self, observable, circuit, initial_state, want_terms):
         args, n_words, n_units, keep = self._inputs(observable, circuit, initial_state, want_terms)
         eng = _native.engine(self.device)
-        res, nt = eng.run(*args)
+        plugin = keep[1]
+        try:
+            res, nt = eng.run(*args)
+        except Exception:
+            if isinstance(plugin, _native.CallbackNoise):
+                plugin.raise_pending()
+            raise
+        if isinstance(plugin, _native.CallbackNoise):
+            plugin.raise_pending()
         self.last_run = res
         terms = eng.terms(n_words) if want_terms else None
         if self.logger is not None:

@@ -102,26 +102,118 @@ def test_weight_only_plugins_match_oracle(gpu_engine, oracle, test_plugins, name
     assert_terms_equal(g.keys, g.coeffs, o.keys, o.coeffs)
 
 
-@pytest.mark.parametrize("case", [c for c in golden_fixture()["cases"]
-                                  if c.get("plugin") in ("uniform_noise", "thermal_decay_noise", "drifting_noise",
-                                                         "depth_dependent_noise")],
-                         ids=lambda c: c["name"])
-def test_reference_weight_only_plugins_golden(gpu_engine, case):
+PLUGIN_CASES = [c for c in golden_fixture()["cases"] if "plugin" in c]
+
+
+@pytest.mark.parametrize("case", PLUGIN_CASES, ids=lambda c: c["name"])
+def test_reference_plugins_golden_and_oracle(gpu_engine, oracle, case):
+    # The reference's nine example plugins on its notebooks' circuit.  The
+    # key-reading noise model and the truncators are asked on the host for
+    # every row / branch (the conformance path); the rest is tabulated.
     so = REF_PLUGINS / f"{case['plugin']}.so"
     if not so.exists():
         pytest.skip("reference example plugins not built")
+    noise = case["plugin_kind"] == "noise"
     p = golden_problem()
-    m = pq.NativeNoiseModel(str(so), case["plugin_config"])
-    g = run_gpu(gpu_engine, p, noise_plugin=m.handle)
+    m = (pq.NativeNoiseModel if noise else pq.NativeTruncator)(str(so), case["plugin_config"])
+    g = run_gpu(gpu_engine, p, **({"noise_plugin": m.handle} if noise else {"truncator": m.handle}))
     assert abs(g.expectation - case["expected"]) <= 1e-12 * abs(case["expected"])
+    h = oracle.load_plugin(so, case["plugin_config"], noise=noise)
+    try:
+        o = oracle.run(p.basis, p.n_units, p.n_words, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets,
+                       diag_state=p.diag, **({"noise_plugin": h} if noise else {"truncator": h}))
+    finally:
+        oracle.lib.pqo_plugin_free(h)
+    assert np.array_equal(g.n_terms, o.n_terms)
+    assert_terms_equal(g.keys, g.coeffs, o.keys, o.coeffs)
 
 
-def test_key_reading_plugins_are_refused(gpu_engine, test_plugins):
-    obs = pq.PauliTermSum({PauliString(0, 1, 4): 1.0})
-    circ = pq.PauliCircuit([pq.PauliRotation(PauliString(1, 0, 4), 0.3)])
-    prop = pq.PauliPropagator(noise=pq.NativeNoiseModel(str(test_plugins["keyed"]), '{"damping": 0.1}'))
-    with pytest.raises(NotImplementedError):
-        prop.expectation_value(obs, circ, 0)
+@pytest.mark.parametrize("seed", [0, 1])
+@pytest.mark.parametrize("kw", [dict(max_weight=4, min_coeff=1e-3), dict(min_coeff=1e-3, min_terms=40), dict()],
+                         ids=["cuts", "floor", "plain"])
+def test_key_reading_noise_and_truncator_match_oracle(gpu_engine, oracle, test_plugins, seed, kw):
+    # Key-reading noise (damps terms on unit 0) and a truncator plugin, with and
+    # without the built-in cuts and a TermBudget floor, on random circuits with
+    # Clifford rotations (no deferral: the noise reads keys).
+    for which in ("noise", "truncator", "both"):
+        p = random_pauli_problem(seed, 8, n_gates=60, **kw)
+        nm = pq.NativeNoiseModel(str(test_plugins["keyed"]), '{"damping": 0.05}')
+        tm = pq.NativeTruncator(str(test_plugins["truncator"]), '{"max_weight": 4}')
+        gk = {}
+        if which in ("noise", "both"):
+            gk["noise_plugin"] = nm.handle
+        if which in ("truncator", "both"):
+            gk["truncator"] = tm.handle
+        g = run_gpu(gpu_engine, p, **gk)
+        hn = oracle.load_plugin(test_plugins["keyed"], '{"damping": 0.05}', noise=True)
+        ht = oracle.load_plugin(test_plugins["truncator"], '{"max_weight": 4}', noise=False)
+        try:
+            ok = {}
+            if which in ("noise", "both"):
+                ok["noise_plugin"] = hn
+            if which in ("truncator", "both"):
+                ok["truncator"] = ht
+            o = run_oracle(oracle, p, **ok)
+        finally:
+            oracle.lib.pqo_plugin_free(hn)
+            oracle.lib.pqo_plugin_free(ht)
+        assert np.array_equal(g.n_terms, o.n_terms), which
+        assert_terms_equal(g.keys, g.coeffs, o.keys, o.coeffs)
+        ok_e, err, tol = expectation_close(g.expectation, o)
+        assert ok_e, which
+
+
+class QubitLocalNoise:
+    """A key-aware Python noise model (damping_factor_term), the same formula as
+    the reference's qubit_local_noise example plugin."""
+
+    def __init__(self, damping, mask):
+        self.damping, self.mask = damping, mask
+        self.calls = 0
+
+    def damping_factor(self, term_weight, active_modes):  # pragma: no cover
+        raise AssertionError("a key-aware model must not fall back to the weight path")
+
+    def damping_factor_term(self, basis_kind, words, n_units, weight):
+        self.calls += 1
+        count = 0
+        for q in range(min(n_units, 64)):
+            if not (self.mask >> q) & 1:
+                continue
+            bit = 2 * q
+            if bit // 64 >= len(words):
+                break
+            if (words[bit // 64] >> (bit % 64)) & 3:
+                count += 1
+        return math.exp(-self.damping * float(count))
+
+
+def test_python_term_hook_matches_the_native_plugin(gpu_engine, oracle):
+    so = REF_PLUGINS / "qubit_local_noise.so"
+    if not so.exists():
+        pytest.skip("reference example plugins not built")
+    wl = workloads.tfim_chain(n=8, steps=3)
+    model = QubitLocalNoise(0.05, 0b10110101)
+    got = pq.PauliPropagator(noise=model, truncation=wl.truncation()).propagate(wl.observable, wl.circuit)
+    assert model.calls > 0
+    p = from_workload(wl)
+    h = oracle.load_plugin(so, '{"damping": 0.05, "mask": 181}', noise=True)
+    try:
+        o = run_oracle(oracle, p, noise_plugin=h)
+    finally:
+        oracle.lib.pqo_plugin_free(h)
+    want = {PauliString.from_key(int(k[0]), 8): c for k, c in zip(o.keys, o.coeffs)}
+    assert dict(got.items()) == want
+
+
+def test_python_term_hook_errors_propagate(gpu_engine):
+    class Broken(QubitLocalNoise):
+        def damping_factor_term(self, basis_kind, words, n_units, weight):
+            raise KeyError("boom")
+
+    wl = workloads.tfim_chain(n=6, steps=2)
+    with pytest.raises(KeyError, match="boom"):
+        pq.PauliPropagator(noise=Broken(0.1, 1)).expectation_value(wl.observable, wl.circuit, 0)
 
 
 # ------------------------------------------------------------ random circuits
