@@ -157,7 +157,20 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def dist_backend() -> str:
+    """NCCL on GPUs; gloo where there is no GPU (the CPU tests of the replica
+    plumbing), or as PQ_DIST_BACKEND says."""
+    b = os.environ.get("PQ_DIST_BACKEND")
+    if b:
+        return b
+    import torch
+
+    return "nccl" if torch.cuda.is_available() else "gloo"
+
+
 def dist_setup():
+    """One process per GPU: the replicas share nothing but the barrier and the
+    max-over-ranks of the timed region (the path does not shard)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -166,8 +179,11 @@ def dist_setup():
         import torch.distributed as dist
         from datetime import timedelta
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        if dist_backend() == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=timedelta(seconds=120))
     return world, rank, local
 
 
@@ -184,9 +200,14 @@ def max_over_ranks(world, value: float) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if dist_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(world: int, units_per_rank: float, seconds_max: float) -> float:
+    """Whole-job throughput of N replicas: all ranks' units over the slowest rank's time."""
+    return world * units_per_rank / seconds_max
 
 
 def gate_bytes(W, rows, anti, children):
@@ -325,7 +346,7 @@ def main_batch(args, world, rank, local):
     clocks = clk.summary()
     dev_s = max_over_ranks(world, dev_ms / 1e3)
     e2e_s = max_over_ranks(world, e2e_s)
-    value = world * terms / dev_s
+    value = replica_value(world, terms, dev_s)
     h2d = sum(p.obs_keys.nbytes + p.obs_coeffs.nbytes + p.gate_keys.nbytes + p.angles.nbytes + p.offsets.nbytes
               + (0 if p.diag is None else p.diag.nbytes) + (0 if p.noise_table is None else p.noise_table.nbytes)
               for p in probs)
@@ -633,7 +654,7 @@ def main():
     clocks = clk.summary()
     dev_s = max_over_ranks(world, dev_ms / 1e3)
     e2e_s = max_over_ranks(world, e2e_s)
-    value = world * terms / dev_s
+    value = replica_value(world, terms, dev_s)
     e2e_value = world * e2e_terms / e2e_s
     # host <-> device bytes per step of pq_run: observable, gates, offsets,
     # state and noise table in; per-gate counts, per-op counters and the
