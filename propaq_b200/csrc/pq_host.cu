@@ -847,24 +847,51 @@ int build_ops(Plan& P, NeedN need_n) {
   return PQ_OK;
 }
 
-// Marks consecutive rotation ops whose (frame-conjugated) generators commute
-// as fused pairs, OP_GATE2 + OP_GATE2_TAIL, which the sweep runs in one pass
-// (gate2_tiles).  Not with a TermBudget floor: its lossless switch reads the
-// live count between the two rotations.  The reverse sweep of the adjoint
-// needs each rotation's own record, so its runs do not fuse.
-void fuse_pairs(Plan& P) {
+// Marks runs of up to FUSE_MAX consecutive rotation ops whose
+// (frame-conjugated) generators pairwise commute and are independent (no
+// subset multiplies to the identity, so a family's members are distinct) as
+// fused groups: a head OP_GATE2 / 3 / 4 and OP_GATE_TAIL ops.  The sweep runs
+// a pair in one pass (gate2_tiles) and larger groups one rotation after the
+// other.  Pairs only: a measured one-pass kernel for 3 and 4 rotations (families
+// of 8 and 16 keys) was slower than pairs on every workload (kicked Ising
+// 46.6 and 52.4 ms against 42.0 ms), its per-family work outweighing the
+// barriers it saves.  Not with a TermBudget floor:
+// its lossless switch reads the live count between rotations; not when the
+// host decides branches; and the adjoint's runs do not fuse (each rotation
+// needs its own record).
+constexpr size_t FUSE_MAX = 2;
+void fuse_groups(Plan& P) {
   if (P.has_floor || P.host_ops) return;
   const size_t gw = gdesc_words(P.W);
-  for (size_t i = 0; i + 1 < P.ops.size(); ++i) {
-    if (P.ops[i].kind != pq::OP_GATE || P.ops[i + 1].kind != pq::OP_GATE) continue;
-    if (P.ops[i + 1].idx != P.ops[i].idx + 1) continue;
-    const u64* g1 = &P.gdesc[P.ops[i].idx * gw];  // GateDesc starts with the generator's words
-    const u64* g2 = &P.gdesc[P.ops[i + 1].idx * gw];
-    if (host_anticommutes(P.alg, P.W, g1, g2)) continue;
-    if (std::equal(g1, g1 + P.W, g2)) continue;  // one axis twice: the family would be a pair
-    P.ops[i].kind = pq::OP_GATE2;
-    P.ops[i + 1].kind = pq::OP_GATE2_TAIL;
-    ++i;
+  const int W = P.W;
+  auto gen = [&](size_t op) { return &P.gdesc[P.ops[op].idx * gw]; };  // GateDesc starts with the generator
+  for (size_t i = 0; i < P.ops.size(); ++i) {
+    if (P.ops[i].kind != pq::OP_GATE) continue;
+    // the XORs of every subset of the group so far (span over GF(2))
+    std::vector<std::vector<u64>> span{std::vector<u64>(W, 0), std::vector<u64>(gen(i), gen(i) + W)};
+    size_t n = 1;
+    while (n < FUSE_MAX && i + n < P.ops.size() && P.ops[i + n].kind == pq::OP_GATE &&
+           P.ops[i + n].idx == P.ops[i].idx + n) {
+      const u64* g = gen(i + n);
+      bool ok = true;
+      for (size_t m = 0; m < n && ok; ++m) ok = !host_anticommutes(P.alg, W, gen(i + m), g);
+      for (const auto& v : span) {  // independent: g is not the product of any subset
+        if (!ok) break;
+        ok = !std::equal(v.begin(), v.end(), g);
+      }
+      if (!ok) break;
+      const size_t before = span.size();
+      for (size_t k = 0; k < before; ++k) {
+        std::vector<u64> v = span[k];
+        for (int w = 0; w < W; ++w) v[w] ^= g[w];
+        span.push_back(v);
+      }
+      ++n;
+    }
+    if (n < 2) continue;
+    P.ops[i].kind = n == 2 ? pq::OP_GATE2 : (n == 3 ? pq::OP_GATE3 : pq::OP_GATE4);
+    for (size_t m = 1; m < n; ++m) P.ops[i + m].kind = pq::OP_GATE_TAIL;
+    i += n - 1;
   }
 }
 
@@ -1293,7 +1320,9 @@ int finish(pq_engine* E, Slot& S, Plan& P, const std::vector<pq::ExpectPartial>&
     switch (P.ops[i].kind) {
       case pq::OP_GATE:
       case pq::OP_GATE2:
-      case pq::OP_GATE2_TAIL:
+      case pq::OP_GATE3:
+      case pq::OP_GATE4:
+      case pq::OP_GATE_TAIL:
         ++res->gate_ops;
         res->gate_ms += op_ms;
         res->sum_rows_gate += n_in;
@@ -1340,7 +1369,7 @@ int run_one(pq_engine* E, const Inputs& in, int W) {
     return PQ_OK;
   };
   if (int rc = build_ops(P, need_n)) return rc;
-  fuse_pairs(P);
+  fuse_groups(P);
   if (int rc = execute_single(E, S, P, grid, &began)) return rc;
   if (!began) cudaEventRecord(E->ev_begin, E->stream);
   std::vector<pq::ExpectPartial> parts;
@@ -1605,7 +1634,7 @@ int run_batch(pq_engine* E, const std::vector<Inputs>& ins, int WM, const pq_bat
       return E->fail(PQ_ERR_UNSUPPORTED, "a batch does not run truncator plugins or key-reading noise; use pq_run");
     if (int rc = setup_slot(E, E->slots[i], plans[i])) return rc;
     if (int rc = build_ops(plans[i], no_sync)) return rc;
-    fuse_pairs(plans[i]);
+    fuse_groups(plans[i]);
     upload_ops(E, E->slots[i], plans[i]);
   }
   const int grid_max = with_words(WM, [&](auto w) {

@@ -119,7 +119,7 @@ struct OpShared {
   u64 n;            // live rows entering the next op
   u32 err;          // SweepState::error
   u32 yield_after;  // SweepState::yield_after
-  u32 extra;        // a word the op asked for (a fused op's count after its first rotation)
+  u32 extra[3];     // words the op asked for (a fused op's rows created by each rotation)
 };
 
 // The barrier between two ops of a sweep.  Thread 0 of each block, once it
@@ -129,7 +129,7 @@ struct OpShared {
 // together into shared memory, one round trip for the block.
 template <class Prefetch>
 __device__ __forceinline__ void op_barrier(SweepState* st, u32& gen, const Grp g_, const u64* n_next, const u32* extra,
-                                           OpShared& os, Prefetch prefetch) {
+                                           u32 n_extra, OpShared& os, Prefetch prefetch) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -145,11 +145,13 @@ __device__ __forceinline__ void op_barrier(SweepState* st, u32& gen, const Grp g
     const u64 n = ld_volatile(n_next);
     const u32 e = *(volatile u32*)&st->error;
     const u32 y = *(volatile u32*)&st->yield_after;
-    const u32 x = extra ? *(const volatile u32*)extra : 0u;
+    u32 x[3] = {0u, 0u, 0u};
+    if (extra)
+      for (u32 i = 0; i < n_extra && i < 3; ++i) x[i] = *(const volatile u32*)(extra + i);
     os.n = n;
     os.err = e;
     os.yield_after = y;
-    os.extra = x;
+    for (int i = 0; i < 3; ++i) os.extra[i] = x[i];
   }
   __syncthreads();
 }
@@ -894,78 +896,79 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
 template <int W, int ALG>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   __shared__ TileSmem sm;
-  __shared__ GateDesc<W> sgate[2];  // op k's generator in slot k & 1
-  __shared__ GateDesc<W> sgate2;    // the second generator of a fused op
-  __shared__ OpDesc sod[2];
+  __shared__ GateDesc<W> sgs[4];  // the op's generator(s)
+  __shared__ OpDesc sod;
   __shared__ OpShared os;
   SweepState* st = a.st;
   u32 gen = *(volatile u32*)&st->bar_gen;
   int cur = (int)a.cur0;
   u32 op = a.op_begin;
   // The live count entering the next op is in n[par]; each op writes
-  // n[par ^ 1].  (Not n[op & 1]: a fused op is two ops.)
+  // n[par ^ 1].  (Not n[op & 1]: a fused op is several ops.)
   u32 par = op & 1u;
-  auto fetch_op = [&](u32 k) {  // thread 0
+  // Thread 0, once every thread is done with the op's shared descriptors.
+  auto fetch_op = [&](u32 k) {
     if (k >= a.op_end) return;
     const OpDesc d = a.ops[k];
-    sod[k & 1] = d;
+    sod = d;
     const GateDesc<W>* gd = reinterpret_cast<const GateDesc<W>*>(a.gates);
-    if (d.kind != OP_NOISE_SCALE && d.kind != OP_NOISE_COMPACT) sgate[k & 1] = gd[d.idx];
-    if (d.kind == OP_GATE2) sgate2 = gd[d.idx + 1];
+    if (d.kind != OP_NOISE_SCALE && d.kind != OP_NOISE_COMPACT)
+      for (u32 i = 0; i < fused_count(d.kind); ++i) sgs[i] = gd[d.idx + i];
   };
   if (threadIdx.x == 0) {
     fetch_op(op);
     os.n = ld_volatile(&st->n[par]);
   }
   __syncthreads();
+  bool stopped = false;  // a capacity stop inside a fused op
   while (op < a.op_end) {
-    OpDesc od = sod[op & 1];
-    // A launch that resumes between the two rotations of a fused op (after a
-    // capacity stop) runs the second as a plain rotation.
-    if (od.kind == OP_GATE2_TAIL) od.kind = OP_GATE;
+    OpDesc od = sod;
+    // A launch that resumes inside a fused group (after a capacity stop) runs
+    // the remaining rotations as plain ones.
+    if (od.kind == OP_GATE_TAIL) od.kind = OP_GATE;
     const u64 N = os.n;
     u64* keys = a.keys[cur];
     double* coeffs = a.coeffs[cur];
     u64* n_out = &st->n[par ^ 1u];
-    const u32 nops = od.kind == OP_GATE2 ? 2u : 1u;
+    const u32 nops = fused_count(od.kind);
     bool split = false;  // a fused op that ran its rotations one after the other
-    if (od.kind == OP_GATE || od.kind == OP_PHASE || od.kind == OP_GATE2) {
+    if (od.kind != OP_NOISE_SCALE && od.kind != OP_NOISE_COMPACT) {
       if (2 * N > a.cap) {  // uniform: every block reads the same N
         if (grp.bid == 0 && threadIdx.x == 0) st->halt = op;
         break;
       }
       if (od.kind == OP_GATE) {
-        gate_op<W, ALG>(a, sgate[op & 1], op, N, keys, coeffs, sm, grp, n_out);
-      } else if (od.kind == OP_GATE2) {
-        if (N == 0) {
-          if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
-        } else if (N <= (u64)grp.nblk * BLOCK * GATE2_TILES_PER_BLOCK && 4 * N <= a.cap) {
-          gate2_tiles<W, ALG>(a, sgate[op & 1], sgate2, op, N, keys, coeffs, sm, grp, n_out);
-        } else {  // many rows: the two rotations one after the other (op + 1 is the second's slot)
-          split = true;
-          gate_op<W, ALG>(a, sgate[op & 1], op, N, keys, coeffs, sm, grp, &st->n_mid);
-          grid_barrier(st, gen, grp);
-          const u64 N1 = ld_volatile(&st->n_mid);
-          if (grp.bid == 0 && threadIdx.x == 0) a.hist[op] = N1;
-          if (2 * N1 > a.cap) {  // stop before the second rotation
+        gate_op<W, ALG>(a, sgs[0], op, N, keys, coeffs, sm, grp, n_out);
+      } else if (od.kind == OP_PHASE) {
+        phase_op<W, ALG>(a, sgs[0], op, N, keys, coeffs, grp);
+        if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, N);
+      } else if (N == 0) {
+        if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
+      } else if (nops == 2 && N <= (u64)grp.nblk * BLOCK * GATE2_TILES_PER_BLOCK && 4 * N <= a.cap) {
+        gate2_tiles<W, ALG>(a, sgs[0], sgs[1], op, N, keys, coeffs, sm, grp, n_out);
+      } else {  // many rows: the rotations one after the other (op + i is rotation i's slot)
+        split = true;
+        u64 Ni = N;
+        for (u32 i = 0; i < nops; ++i) {
+          if (i > 0 && 2 * Ni > a.cap) {  // stop before rotation i
             if (grp.bid == 0 && threadIdx.x == 0) {
-              st->n[par] = N1;  // read as the next op's count (nobody reads n[par] during this op)
-              st->halt = op + 1;
-              if (N1 > st->peak) st->peak = N1;
-              if (a.stamps) {
-                u64 t;
-                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-                a.stamps[op] = t;
-              }
+              st->n[par] = Ni;  // read as the next op's count (nobody reads n[par] during this op)
+              st->halt = op + i;
+              if (Ni > st->peak) st->peak = Ni;
             }
-            ++op;
+            op += i;
+            stopped = true;
             break;
           }
-          gate_op<W, ALG>(a, sgate2, op + 1, N1, keys, coeffs, sm, grp, n_out);
+          u64* out_i = i + 1 == nops ? n_out : &st->n_mid[i & 1];
+          gate_op<W, ALG>(a, sgs[i], op + i, Ni, keys, coeffs, sm, grp, out_i);
+          if (i + 1 < nops) {
+            grid_barrier(st, gen, grp);
+            Ni = ld_volatile(out_i);
+            if (grp.bid == 0 && threadIdx.x == 0) a.hist[op + i] = Ni;
+          }
         }
-      } else {
-        phase_op<W, ALG>(a, sgate[op & 1], op, N, keys, coeffs, grp);
-        if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, N);
+        if (stopped) break;
       }
     } else if (od.kind == OP_NOISE_SCALE) {
       noise_scale_op<W, ALG>(a, a.tables + (u64)od.idx * a.table_len, N, keys, coeffs, grp);
@@ -985,7 +988,8 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     // the same branch (a block reading late sees a later op and goes on).
     if (a.idle_blocks && grp.bid == 0 && threadIdx.x == 0 && *(volatile u32*)a.idle_blocks >= a.yield_at)
       *(volatile u32*)&st->yield_after = op + 1;
-    op_barrier(st, gen, grp, n_out, nops == 2 ? a.tickets + op : nullptr, os, [&] { fetch_op(op + nops); });
+    op_barrier(st, gen, grp, n_out, nops > 1 && !split ? a.tickets + op : nullptr, nops - 1, os,
+               [&] { fetch_op(op + nops); });
     par ^= 1u;
     if (os.err) {
       op += nops;
@@ -994,13 +998,18 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     if (grp.bid == 0 && threadIdx.x == 0) {
       const u64 n_new = os.n;
       a.hist[op + nops - 1] = n_new;
-      if (nops == 2 && !split) a.hist[op] = N + os.extra;
+      if (nops > 1 && !split) {  // counts after each rotation of the group but the last
+        u64 acc = N;
+        for (u32 i = 0; i + 1 < nops; ++i) {
+          acc += os.extra[i];
+          a.hist[op + i] = acc;
+        }
+      }
       if (n_new > st->peak) st->peak = n_new;
       if (a.stamps) {
         u64 t;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        a.stamps[op] = t;
-        if (nops == 2) a.stamps[op + 1] = t;
+        for (u32 i = 0; i < nops; ++i) a.stamps[op + i] = t;
       }
     }
     const bool stop = a.idle_blocks && os.yield_after == op + 1;

@@ -13,9 +13,16 @@ enum OpKind : u32 {
   OP_PHASE = 1,          // |sin| < eps: scale the anticommuting rows by cos
   OP_NOISE_SCALE = 2,    // damp every row by its weight's factor
   OP_NOISE_COMPACT = 3,  // damp, then reclaim: filter + compact + re-insert
-  OP_GATE2 = 4,          // this rotation and the next (whose generators commute) in one pass
-  OP_GATE2_TAIL = 5,     // the second rotation of an OP_GATE2: run by it, skipped by the sweep
+  OP_GATE2 = 4,          // this rotation and the next 1 / 2 / 3 (whose generators commute)
+  OP_GATE_TAIL = 5,      // a later rotation of such a group: run by its head, skipped by the sweep
+  OP_GATE3 = 6,
+  OP_GATE4 = 7,
 };
+
+// Rotations run by an op: 2 to 4 for a fused group's head, else 1.
+__host__ __device__ inline u32 fused_count(u32 kind) {
+  return kind == OP_GATE2 ? 2u : (kind == OP_GATE3 ? 3u : (kind == OP_GATE4 ? 4u : 1u));
+}
 
 struct OpDesc {
   u32 kind;
@@ -32,7 +39,7 @@ struct GateDesc {
 struct SweepState {
   u64 n[2];       // live rows: op k reads n[k & 1], writes n[(k + 1) & 1]
   u64 peak;       // largest live count the sweeps have seen
-  u64 n_mid;      // live rows between the two rotations of a fused op run one after the other
+  u64 n_mid[2];   // live rows between the rotations of a fused op run one after the other
   u32 halt;       // op at which a sweep stopped for capacity, or NOT_HALTED
   u32 error;      // ERR_* bits
   u32 cur;        // row buffer holding the live rows when the sweep ended
