@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "kicked_ising_small", "majorana", "majorana_small", "tfim", "batch", "adjoint"])
+    ap.add_argument("--workload", default="kicked_ising", choices=["kicked_ising", "kicked_ising_small", "majorana", "majorana_small", "tfim", "batch",
+                             "batch_small", "adjoint", "adjoint_small"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="sweep blocks per SM (0 = as many as fit)")
@@ -242,7 +243,10 @@ def main_batch(args, world, rank, local):
 
     from propaq_b200 import workloads
 
-    wls = workloads.kicked_ising_batch(64, seed=0)
+    if args.workload == "batch_small":  # profiling case: 16 instances, 40..60 qubits, 4..6 steps
+        wls = workloads.kicked_ising_batch(16, seed=0, n_range=(40, 60), steps_range=(4, 6))
+    else:
+        wls = workloads.kicked_ising_batch(64, seed=0)
     probs = [from_workload(w) for w in wls]
     cores = os.cpu_count() or 1
     desc = ("64 kicked-Ising instances, n ~ U{40..100} on the most-square open grid, steps ~ U{8..20}, "
@@ -250,7 +254,8 @@ def main_batch(args, world, rank, local):
     base_line = {"metric": "terms/s", "unit": "terms/s", "n_gpus": args.gpus, "steps": args.steps,
                  "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                  "dtype": "f64", "data": "synthetic (seeded; no dataset)",
-                 "config": {"workload": desc, "name": "kicked_ising_batch64_seed0", "instances": len(probs),
+                 "config": {"workload": desc if args.workload == "batch" else "profiling case: " + args.workload,
+                            "name": f"kicked_ising_batch{len(probs)}_seed0", "instances": len(probs),
                             "gates": int(sum(len(p.angles) for p in probs)),
                             "parallelism": f"replicas x{world}", "l2": "flushed between steps"}}
     if args.impl == "reference":
@@ -398,7 +403,8 @@ def main_adjoint(args, world, rank, local):
     from propaq_b200 import PauliPropagator, workloads
     from propaq_b200.adjoint import ParametrizedExpectation
 
-    wl = workloads.hardware_efficient()
+    # adjoint_small is the profiling case: 20 qubits, 4 layers
+    wl = workloads.hardware_efficient(20, 4) if args.workload == "adjoint_small" else workloads.hardware_efficient()
     th = wl.meta["theta"]
     desc = ("hardware-efficient ansatz 50 qubits, 12 layers of RY+RZ on all + CNOT ladder (Z_c(pi/2), X_t(pi/2), "
             "Z_cX_t(-pi/2)), 1200 angles ~ N(0,0.1), sum Z_i Z_i+1, |0..0>, w<=8, |c|>=1e-5, no noise")
@@ -406,7 +412,8 @@ def main_adjoint(args, world, rank, local):
     base_line = {"metric": "gradients/s", "unit": "gradients/s", "n_gpus": args.gpus, "steps": args.steps,
                  "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                  "dtype": "f64", "data": "synthetic (seeded; no dataset)",
-                 "config": {"workload": desc, "name": wl.name, "n_units": 50, "angles": len(th),
+                 "config": {"workload": desc if args.workload == "adjoint" else "profiling case: " + wl.name,
+                            "name": wl.name, "n_units": wl.n_units, "angles": len(th),
                             "gates": len(wl.circuit.rotations), "checkpoint_layers": args.checkpoint_layers,
                             "parallelism": f"replicas x{world}", "l2": "flushed between steps"}}
     spec_cpu = ParametrizedExpectation(PauliPropagator(truncation=wl.truncation()), wl.observable, wl.circuit,
@@ -526,9 +533,9 @@ def oracle_load():
 def main():
     args = parse()
     world, rank, local = dist_setup()
-    if args.workload == "batch":
+    if args.workload in ("batch", "batch_small"):
         return main_batch(args, world, rank, local)
-    if args.workload == "adjoint":
+    if args.workload in ("adjoint", "adjoint_small"):
         return main_adjoint(args, world, rank, local)
     wl, desc = make_workload(args.workload)
     cores = os.cpu_count() or 1
