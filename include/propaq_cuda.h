@@ -201,19 +201,22 @@ int pq_run_batch(pq_engine* engine, const pq_instance* instances, size_t n, cons
  * parameter sweep is surrogate evaluation (crates/surrogate/src/model.rs:63-107);
  * it backs a torch.autograd.Function over the propagators.
  *
- * Arguments as pq_run; diag_state is required.  The forward run is cut into
- * segments of checkpoint_layers layers (0 = one segment) whose starting terms
- * are kept; the reverse pass re-runs one segment at a time while recording
- * its branches, so device memory grows with one segment's work, not the whole
- * run's.  Gates deferred into the Clifford frame (fixed Clifford rotations)
- * get NaN.  A TermBudget floor with a weight cut and a weight-changing
- * Clifford rotation is refused (PQ_ERR_UNSUPPORTED).  out->device_ms covers
- * both passes. */
+ * Arguments as pq_run; diag_state is required.  The forward run records what
+ * the reverse pass needs into a pool of record_bytes of device memory (0 =
+ * 40% of the free memory, at most 48 GB): 12 bytes per row entering each
+ * rotation.  When it all fits, one reverse sweep follows.  Otherwise the
+ * forward run's terms at the start of every checkpoint_layers layers (0 = one
+ * segment) are used to re-run one segment at a time while recording.  Gates
+ * deferred into the Clifford frame (fixed Clifford rotations) get NaN.  A
+ * TermBudget floor with a weight cut and a weight-changing Clifford rotation
+ * is refused (PQ_ERR_UNSUPPORTED), as are truncator plugins and key-reading
+ * noise.  out->device_ms covers both passes. */
 int pq_run_adjoint(pq_engine* engine, const pq_run_config* cfg, const uint64_t* obs_words,
                    const double* obs_coeffs, size_t n_obs, const uint64_t* gate_words,
                    const double* gate_angles, size_t n_gates, const uint32_t* layer_offsets,
                    size_t n_layers, const uint64_t* diag_state, size_t diag_words,
-                   uint32_t checkpoint_layers, double* grad, uint64_t* n_terms_out, pq_result* out);
+                   uint32_t checkpoint_layers, uint64_t record_bytes, double* grad,
+                   uint64_t* n_terms_out, pq_result* out);
 
 /* Final terms of instance `index` of the last batch (index 0 after pq_run),
  * as pq_result_terms. */

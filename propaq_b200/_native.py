@@ -126,7 +126,7 @@ _SIGNATURES = {
     "pq_run_batch": (ctypes.c_int, [_V, ctypes.POINTER(Instance), _Z, ctypes.POINTER(BatchTuning)]),
     "pq_result_terms_at": (_Z, [_V, _Z, _V, _V, _Z]),
     "pq_run_adjoint": (ctypes.c_int, [_V, ctypes.POINTER(RunConfig), _V, _V, _Z, _V, _V, _Z, _V, _Z, _V, _Z, _U32,
-                                      _V, _V, ctypes.POINTER(RunResult)]),
+                                      ctypes.c_uint64, _V, _V, ctypes.POINTER(RunResult)]),
     "pq_plugin_load_noise": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_V),
                                             ctypes.c_char_p, _Z]),
     "pq_plugin_load_truncator": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_V),
@@ -213,7 +213,7 @@ class Engine:
         return res, nt
 
     def run_adjoint(self, cfg: RunConfig, obs_words, obs_coeffs, gate_words, gate_angles, layer_offsets,
-                    diag_state, checkpoint_layers: int = 0):
+                    diag_state, checkpoint_layers: int = 0, record_bytes: int = 0):
         """Runs pq_run_adjoint; returns (RunResult, n_terms array, dE/d gate_angles)."""
         obs_words = np.ascontiguousarray(obs_words, dtype=np.uint64)
         obs_coeffs = np.ascontiguousarray(obs_coeffs, dtype=np.float64)
@@ -228,7 +228,8 @@ class Engine:
         with self.lock:
             rc = lib().pq_run_adjoint(self._h, ctypes.byref(cfg), _ptr(obs_words), _ptr(obs_coeffs), len(obs_coeffs),
                                       _ptr(gate_words), _ptr(gate_angles), n_gates, _ptr(layer_offsets),
-                                      len(layer_offsets) - 1, _ptr(diag), len(diag), checkpoint_layers, _ptr(grad),
+                                      len(layer_offsets) - 1, _ptr(diag), len(diag), checkpoint_layers,
+                                      record_bytes, _ptr(grad),
                                       _ptr(nt), ctypes.byref(res))
             if rc != PQ_OK:
                 raise_for(rc, lib().pq_engine_last_error(self._h).decode(errors="replace"))

@@ -4,10 +4,12 @@ E(theta) = <s| U(theta)^dag O U(theta) |s> for a circuit whose rotation k
 (circuit order) has angle  scale[k] * theta[index[k]]  (index[k] = -1 keeps
 the circuit's own angle, e.g. the fixed pieces of a CNOT).
 
-The gradient comes from pq_run_adjoint: one forward propagation with a
-checkpoint of the live terms every `checkpoint_layers` circuit layers, then a
-reverse sweep on the GPU that carries dE/dc back through every op with the
-forward run's truncation decisions held fixed.  It is the exact derivative of
+The gradient comes from pq_run_adjoint: one forward propagation that records
+every op (and keeps the live terms every `checkpoint_layers` circuit layers),
+then a reverse sweep on the GPU that carries dE/dc back through every op with
+the forward run's truncation decisions held fixed.  `record_bytes` bounds the
+device memory of the records (0: 40% of the free memory); past it, segments
+are re-run to record them.  It is the exact derivative of
 the function the engine evaluates wherever those decisions do not change
 under a small change of theta (and the exact derivative of the untruncated
 expectation when nothing is truncated).
@@ -52,13 +54,14 @@ class ParametrizedExpectation:
     parameter vector."""
 
     def __init__(self, propagator, observable, circuit, param_index, param_scale=None, initial_state=0,
-                 checkpoint_layers: int = 3):
+                 checkpoint_layers: int = 3, record_bytes: int = 0):
         args, n_words, n_units, keep = propagator._inputs(observable, circuit, initial_state, False)
         self._args = list(args)
         self._keep = keep
         self.propagator = propagator
         self.device = propagator.device
         self.checkpoint_layers = int(checkpoint_layers)
+        self.record_bytes = int(record_bytes)
         self.n_words = n_words
         order = _heisenberg_order(circuit)
         idx = np.asarray(param_index, dtype=np.int64)
@@ -93,7 +96,8 @@ class ParametrizedExpectation:
     def value_and_grad(self, theta):
         """(E, dE/dtheta) from one forward and one reverse pass."""
         res, _, g_gate = _native.engine(self.device).run_adjoint(*self._call_args(theta),
-                                                                 checkpoint_layers=self.checkpoint_layers)
+                                                                 checkpoint_layers=self.checkpoint_layers,
+                                                                 record_bytes=self.record_bytes)
         self.propagator.last_run = res
         return float(res.expectation_value), self._chain(g_gate)
 

@@ -637,6 +637,8 @@ struct Plan {
   Tableau frame{0, 1, 0};
   long last_op = -1;
   size_t done = 0, uploaded_ops = 0, uploaded_gdesc = 0;
+  u64 rec_next = 0, rec_key_next = 0;  // adjoint recording: next free slots of the pool
+  u32 rec_full = 0;
   u64 n_live = 0, peak = 0;
   double sweep_ms = 0;
   u64 sweep_launches = 0;
@@ -914,8 +916,9 @@ struct Recording {
   u32* idx = nullptr;
   double* coef = nullptr;
   u64* keys = nullptr;
-  u64* off = nullptr;
+  u64* off = nullptr;      // written by the sweep, per op
   u64* key_off = nullptr;
+  u64 cap = 0, key_cap = 0;  // elements of idx / coef, rows of keys
 };
 
 // Per-row decisions made on the host for one op (device pointers, or null).
@@ -948,6 +951,8 @@ pq::SweepArgs sweep_args(Slot& S, const Plan& P, pq::SweepState* st, u32 blk_beg
     a.rec_keys = rec->keys;
     a.rec_off = rec->off;
     a.rec_key_off = rec->key_off;
+    a.rec_cap = rec->cap;
+    a.rec_key_cap = rec->key_cap;
   }
   a.cur0 = (u32)S.cur;
   a.epoch_base = S.epoch_base;
@@ -978,6 +983,9 @@ pq::SweepState fresh_state(const Plan& P) {
   s.n[P.done & 1] = P.n_live;
   s.peak = P.peak;
   s.halt = pq::NOT_HALTED;
+  s.rec_next = P.rec_next;
+  s.rec_key_next = P.rec_key_next;
+  s.rec_full = P.rec_full;
   return s;
 }
 
@@ -994,6 +1002,9 @@ int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
   P.done = h.end_op;
   P.n_live = h.n[P.done & 1];
   P.peak = std::max(P.peak, h.peak);
+  P.rec_next = h.rec_next;
+  P.rec_key_next = h.rec_key_next;
+  P.rec_full = h.rec_full;
   ++P.sweep_launches;
   if (h.halt != pq::NOT_HALTED) {
     u64 ncap = next_pow2(std::max<u64>(4 * P.n_live, 2 * S.cap));
@@ -1399,15 +1410,17 @@ struct RunBuffers {
 };
 
 // Expectation value and dE/d(angle) of every gate with the truncation
-// decisions of the forward run held fixed.  The forward run is split into
-// segments of ckpt_layers layers and keeps the live terms at the start of
-// each.  Then, last segment first, it restores a segment's start, runs the
-// segment again while recording each op's sin branches and reclaim maps
-// (SweepArgs::rec_idx), and runs the reverse sweep over it (adjoint_kernel),
-// which carries dE/dc back to the segment's start.  Device memory: the
-// checkpoints, plus 12 bytes per row entering each op of one segment (and
-// 8W + 4 per row entering each reclaim).
-int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, double* grad_out) {
+// decisions of the forward run held fixed.  The forward run records each op
+// (SweepArgs::rec_idx: sin-branch partners, pre-op coefficients, reclaim maps
+// and key snapshots) into a pool of record_bytes (0: 40% of the free device
+// memory, at most 48 GB) and keeps the live terms at the start of every
+// segment of ckpt_layers layers.  If every op fit, one reverse sweep
+// (adjoint_kernel) carries dE/dc from the final rows back to the observable.
+// If the pool ran out, the reverse pass goes segment by segment, last first:
+// restore the segment's start, run it again recording from the start of the
+// pool, sweep it in reverse.  Records take 12 bytes per row entering each op
+// (plus 8W per row entering a reclaim).
+int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, u64 record_bytes, double* grad_out) {
   if (!in.diag) return E->fail(PQ_ERR_INVALID, "the gradient needs an initial state");
   if (int rc = E->ensure_slots(1)) return rc;
   Slot& S = E->slots[0];
@@ -1440,11 +1453,27 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, double* 
   RunBuffers mem;
   cudaError_t e;
 
-  // Forward, keeping each segment's starting terms.
+  // The record pool: a share of the free device memory, split between the
+  // per-row records (12 B an element) and reclaim key snapshots.
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t budget = record_bytes ? (size_t)record_bytes : std::min<size_t>(free_b / 5 * 2, (size_t)48 << 30);
+  Recording rec;
+  rec.cap = std::max<u64>(budget / 100 * 85 / 12, 1);
+  rec.key_cap = std::max<u64>(budget / 100 * 15 / (8 * (size_t)W), 1);
+  if ((e = mem.alloc(&rec.idx, rec.cap)) != cudaSuccess || (e = mem.alloc(&rec.coef, rec.cap)) != cudaSuccess ||
+      (e = mem.alloc(&rec.keys, rec.key_cap * W)) != cudaSuccess || (e = mem.alloc(&rec.off, n_ops)) != cudaSuccess ||
+      (e = mem.alloc(&rec.key_off, n_ops)) != cudaSuccess)
+    return E->cuda_fail(e, "gradient record pool");
+
+  // Forward, keeping each segment's starting terms and recording every op
+  // while the pool lasts.
   std::vector<u64*> ck_keys(n_seg, nullptr);
   std::vector<double*> ck_coeffs(n_seg, nullptr);
   std::vector<u64> ck_n(n_seg, 0);
   bool began = false;
+  P.rec_next = P.rec_key_next = 0;
+  P.rec_full = 0;
   for (size_t s = 0; s < n_seg; ++s) {
     ck_n[s] = P.n_live;
     if ((e = mem.alloc(&ck_keys[s], ck_n[s] * W)) != cudaSuccess ||
@@ -1452,8 +1481,9 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, double* 
       return E->cuda_fail(e, "checkpoint");
     cudaMemcpyAsync(ck_keys[s], S.keys[S.cur], ck_n[s] * W * 8, cudaMemcpyDeviceToDevice, E->stream);
     cudaMemcpyAsync(ck_coeffs[s], S.coeffs[S.cur], ck_n[s] * 8, cudaMemcpyDeviceToDevice, E->stream);
-    if (int rc = execute_single(E, S, P, grid, &began, seg[s + 1])) return rc;
+    if (int rc = execute_single(E, S, P, grid, &began, seg[s + 1], &rec)) return rc;
   }
+  const bool recorded_all = !P.rec_full;
   if (!began) cudaEventRecord(E->ev_begin, E->stream);
   std::vector<pq::ExpectPartial> parts;
   if (int rc = finalize(E, S, P, &parts)) return rc;
@@ -1461,46 +1491,24 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, double* 
   if (int rc = finish(E, S, P, parts)) return rc;
   const u64 n_fin = P.n_live;
 
-  // Rows entering each op, recording offsets, gate -> op map.
-  std::vector<u64> hist(n_ops), n_in(n_ops), off(n_ops, 0), koff(n_ops, 0);
+  // Rows entering each op, gate -> op map, adjoint buffers.
+  std::vector<u64> hist(n_ops), n_in(n_ops), koff(n_ops, 0);
   if (n_ops) cudaMemcpy(hist.data(), S.hist, n_ops * 8, cudaMemcpyDeviceToHost);
   for (size_t k = 0; k < n_ops; ++k) n_in[k] = k ? hist[k - 1] : P.n0;
-  size_t max_rec = 0, max_krec = 0;
-  for (size_t s = 0; s < n_seg; ++s) {
-    size_t tot = 0, ktot = 0;
-    for (size_t k = seg[s]; k < seg[s + 1]; ++k) {
-      if (P.ops[k].kind != pq::OP_NOISE_SCALE) {
-        off[k] = tot;
-        tot += n_in[k];
-      }
-      if (P.ops[k].kind == pq::OP_NOISE_COMPACT) {
-        koff[k] = ktot;
-        ktot += n_in[k];
-      }
-    }
-    max_rec = std::max(max_rec, tot);
-    max_krec = std::max(max_krec, ktot);
-  }
   std::vector<long long> gate_ops(in.n_gates);
   for (size_t g = 0; g < in.n_gates; ++g) gate_ops[g] = P.gate_own[g] ? P.gate_op[g] : -1;
-  Recording rec;
   double* lam[2] = {nullptr, nullptr};
   double* grad_part = nullptr;
   double* d_grad = nullptr;
   u64* d_n_in = nullptr;
   long long* d_gate_ops = nullptr;
   const u64** d_ksrc = nullptr;
-  if ((e = mem.alloc(&rec.idx, max_rec)) != cudaSuccess || (e = mem.alloc(&rec.coef, max_rec)) != cudaSuccess ||
-      (e = mem.alloc(&rec.keys, max_krec * W)) != cudaSuccess || (e = mem.alloc(&rec.off, n_ops)) != cudaSuccess ||
-      (e = mem.alloc(&rec.key_off, n_ops)) != cudaSuccess || (e = mem.alloc(&lam[0], S.cap)) != cudaSuccess ||
-      (e = mem.alloc(&lam[1], S.cap)) != cudaSuccess ||
+  if ((e = mem.alloc(&lam[0], S.cap)) != cudaSuccess || (e = mem.alloc(&lam[1], S.cap)) != cudaSuccess ||
       (e = mem.alloc(&grad_part, n_ops * (size_t)agrid)) != cudaSuccess ||
       (e = mem.alloc(&d_grad, in.n_gates)) != cudaSuccess || (e = mem.alloc(&d_n_in, n_ops)) != cudaSuccess ||
       (e = mem.alloc(&d_gate_ops, in.n_gates)) != cudaSuccess || (e = mem.alloc(&d_ksrc, n_ops)) != cudaSuccess)
     return E->cuda_fail(e, "adjoint buffers");
   if (n_ops) {
-    cudaMemcpyAsync(rec.off, off.data(), n_ops * 8, cudaMemcpyHostToDevice, E->stream);
-    cudaMemcpyAsync(rec.key_off, koff.data(), n_ops * 8, cudaMemcpyHostToDevice, E->stream);
     cudaMemcpyAsync(d_n_in, n_in.data(), n_ops * 8, cudaMemcpyHostToDevice, E->stream);
     cudaMemsetAsync(grad_part, 0, n_ops * (size_t)agrid * 8, E->stream);
   }
@@ -1518,27 +1526,21 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, double* 
   if (e != cudaSuccess) return E->cuda_fail(e, "adjoint seed");
   int lam_cur = 0;
 
-  // Reverse, one segment at a time.
-  for (size_t s = n_seg; s-- > 0;) {
-    if (seg[s] == seg[s + 1]) continue;
-    if (ck_n[s]) {
-      cudaMemcpyAsync(S.keys[0], ck_keys[s], ck_n[s] * W * 8, cudaMemcpyDeviceToDevice, E->stream);
-      cudaMemcpyAsync(S.coeffs[0], ck_coeffs[s], ck_n[s] * 8, cudaMemcpyDeviceToDevice, E->stream);
-    }
-    S.cur = 0;
-    if (int rc = E->rebuild_table(S, ck_n[s])) return rc;
-    P.done = seg[s];
-    P.n_live = ck_n[s];
-    if (int rc = execute_single(E, S, P, grid, &began, seg[s + 1], &rec)) return rc;
-    // Keys of each op's input rows: the snapshot of the next reclaim of the
-    // segment (rows only grow until then), else the segment's last buffer.
-    std::vector<const u64*> ksrc(seg[s + 1] - seg[s]);
-    const u64* next = S.keys[S.cur];
-    for (size_t k = seg[s + 1]; k-- > seg[s];) {
+  // The reverse sweep over ops [b, e): keys of each op's input rows are the
+  // snapshot of the next reclaim (rows only grow until then), else the buffer
+  // the rows ended in.
+  auto reverse = [&](size_t b, size_t end_op, const u64* last_keys) -> int {
+    if (b == end_op) return PQ_OK;
+    cudaMemcpyAsync(koff.data() + b, rec.key_off + b, (end_op - b) * 8, cudaMemcpyDeviceToHost, E->stream);
+    cudaError_t ee;
+    if ((ee = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(ee, "record offsets");
+    std::vector<const u64*> ksrc(end_op - b);
+    const u64* next = last_keys;
+    for (size_t k = end_op; k-- > b;) {
       if (P.ops[k].kind == pq::OP_NOISE_COMPACT) next = rec.keys + koff[k] * W;
-      ksrc[k - seg[s]] = next;
+      ksrc[k - b] = next;
     }
-    cudaMemcpyAsync(d_ksrc + seg[s], ksrc.data(), ksrc.size() * sizeof(u64*), cudaMemcpyHostToDevice, E->stream);
+    cudaMemcpyAsync(d_ksrc + b, ksrc.data(), ksrc.size() * sizeof(u64*), cudaMemcpyHostToDevice, E->stream);
     E->h_states[0] = pq::SweepState{};
     cudaMemcpyAsync(E->d_states, E->h_states, sizeof(pq::SweepState), cudaMemcpyHostToDevice, E->stream);
     pq::AdjointArgs aa{};
@@ -1547,8 +1549,8 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, double* 
     aa.tables = S.d_tables;
     aa.table_len = (u32)P.tlen;
     aa.n_units = P.n_units;
-    aa.op_begin = (u32)seg[s];
-    aa.op_end = (u32)seg[s + 1];
+    aa.op_begin = (u32)b;
+    aa.op_end = (u32)end_op;
     aa.cur0 = (u32)lam_cur;
     aa.n_in = d_n_in;
     aa.rec_idx = rec.idx;
@@ -1560,18 +1562,45 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, double* 
     aa.grad_part = grad_part;
     aa.st = E->d_states;
     ++E->launches;
-    e = with_words(W, [&](auto w) {
+    ee = with_words(W, [&](auto w) {
       constexpr int WW = decltype(w)::value;
       return ALG == 0 ? pq::launch_adjoint<WW, 0>(aa, agrid, E->stream) : pq::launch_adjoint<WW, 1>(aa, agrid, E->stream);
     });
-    if (e != cudaSuccess) return E->cuda_fail(e, "adjoint launch");
+    if (ee != cudaSuccess) return E->cuda_fail(ee, "adjoint launch");
     cudaMemcpyAsync(E->h_states, E->d_states, sizeof(pq::SweepState), cudaMemcpyDeviceToHost, E->stream);
-    if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(e, "adjoint");
+    if ((ee = cudaStreamSynchronize(E->stream)) != cudaSuccess) return E->cuda_fail(ee, "adjoint");
     if (E->h_states[0].error & pq::ERR_BARRIER_TIMEOUT)
       return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a grid barrier wait expired on the device");
-    if (E->h_states[0].error) return E->fail(PQ_ERR_CUDA, "device reported error bits " +
-                                                             std::to_string(E->h_states[0].error));
+    if (E->h_states[0].error)
+      return E->fail(PQ_ERR_CUDA, "device reported error bits " + std::to_string(E->h_states[0].error));
     lam_cur = (int)E->h_states[0].cur;
+    return PQ_OK;
+  };
+
+  if (recorded_all) {
+    // Every op was recorded in the forward pass: one reverse sweep, no replay.
+    if (int rc = reverse(0, n_ops, S.keys[S.cur])) return rc;
+  } else {
+    // The pool ran out: last segment first, restore its start, run it again
+    // recording from the start of the pool, then sweep it in reverse.
+    for (size_t sg = n_seg; sg-- > 0;) {
+      if (seg[sg] == seg[sg + 1]) continue;
+      if (ck_n[sg]) {
+        cudaMemcpyAsync(S.keys[0], ck_keys[sg], ck_n[sg] * W * 8, cudaMemcpyDeviceToDevice, E->stream);
+        cudaMemcpyAsync(S.coeffs[0], ck_coeffs[sg], ck_n[sg] * 8, cudaMemcpyDeviceToDevice, E->stream);
+      }
+      S.cur = 0;
+      if (int rc = E->rebuild_table(S, ck_n[sg])) return rc;
+      P.done = seg[sg];
+      P.n_live = ck_n[sg];
+      P.rec_next = P.rec_key_next = 0;
+      P.rec_full = 0;
+      if (int rc = execute_single(E, S, P, grid, &began, seg[sg + 1], &rec)) return rc;
+      if (P.rec_full)
+        return E->fail(PQ_ERR_OOM, "one segment's gradient records exceed the device memory set aside for them; "
+                                   "use fewer checkpoint layers");
+      if (int rc = reverse(seg[sg], seg[sg + 1], S.keys[S.cur])) return rc;
+    }
   }
   ++E->launches;
   if ((e = pq::launch_grad_reduce(grad_part, agrid, d_gate_ops, in.n_gates, d_grad, E->stream)) != cudaSuccess)
@@ -1827,7 +1856,8 @@ int pq_run_batch(pq_engine* E, const pq_instance* insts, size_t n, const pq_batc
 
 int pq_run_adjoint(pq_engine* E, const pq_run_config* cfg, const uint64_t* ow, const double* oc, size_t no,
                    const uint64_t* gw, const double* ga, size_t ng, const uint32_t* lo, size_t nl, const uint64_t* d,
-                   size_t nd, uint32_t checkpoint_layers, double* grad, uint64_t* nt, pq_result* r) {
+                   size_t nd, uint32_t checkpoint_layers, uint64_t record_bytes, double* grad, uint64_t* nt,
+                   pq_result* r) {
   if (!E || !cfg || !r || (ng && !grad)) return PQ_ERR_INVALID;
   std::memset(r, 0, sizeof(*r));
   E->err.clear();
@@ -1836,7 +1866,7 @@ int pq_run_adjoint(pq_engine* E, const pq_run_config* cfg, const uint64_t* ow, c
   if (cudaSetDevice(E->device) != cudaSuccess) return E->fail(PQ_ERR_CUDA, "cudaSetDevice failed");
   const u64 l0 = E->launches;
   const Inputs in{cfg, K(ow), oc, no, K(gw), ga, ng, lo, nl, K(d), nd, reinterpret_cast<u64*>(nt), r, W};
-  const int rc = run_adjoint(E, in, W, checkpoint_layers, grad);
+  const int rc = run_adjoint(E, in, W, checkpoint_layers, record_bytes, grad);
   r->gpu_launches = E->launches - l0;
   return rc;
 }

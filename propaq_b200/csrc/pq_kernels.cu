@@ -339,6 +339,8 @@ struct TileSmem {
   u32 tile;
   u32 excl;
   u32 cnt[32];  // item-major per-warp counts, then their exclusive prefixes
+  u32 rec_on;   // adjoint recording of the running op (see SweepArgs::rec_idx)
+  u64 rec_base, rec_key_base;
 };
 
 // Item-major block scan of IT flags per thread, then the look-back.  Leaves
@@ -376,14 +378,14 @@ __device__ __forceinline__ void tile_scan(u32 flags, unsigned* masks, TileSmem& 
 // Adjoint recording of one gate's sin branches (see SweepArgs::rec_idx).  A
 // source without a partner row records REC_NONE here; its child's row
 // replaces it once the child is placed.
-__device__ __forceinline__ void record_single(const SweepArgs& a, u32 op, u64 r, double c) {
-  const u64 o = a.rec_off[op];
+__device__ __forceinline__ void record_single(const SweepArgs& a, const TileSmem& sm, u64 r, double c) {
+  const u64 o = sm.rec_base;
   a.rec_coef[o + r] = c;
   a.rec_idx[o + r] = REC_NONE;
 }
-__device__ __forceinline__ void record_pair(const SweepArgs& a, u32 op, u64 r, u64 j, double c, double cj, bool to_j,
-                                            bool to_i) {
-  const u64 o = a.rec_off[op];
+__device__ __forceinline__ void record_pair(const SweepArgs& a, const TileSmem& sm, u64 r, u64 j, double c, double cj,
+                                            bool to_j, bool to_i) {
+  const u64 o = sm.rec_base;
   a.rec_coef[o + r] = c;
   a.rec_coef[o + j] = cj;
   a.rec_idx[o + r] = to_j ? (u32)j : REC_NONE;
@@ -473,7 +475,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
           bval[k] = bi;
           slot[k] = claim_slot<W>(q, a.table, a.table_mask, &st->error);
         }
-        if (a.rec_idx) record_single(a, op, r, c[k]);
+        if (sm.rec_on) record_single(a, sm, r, c[k]);
       } else {
         const double bj = __dmul_rn(__dmul_rn(cj[k], sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
         const int sj = a.host_state ? (int)a.host_state[j[k]] : state(cj[k], key[k]);
@@ -485,7 +487,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
         if (to_j) nj = __dadd_rn(nj, bi);
         coeffs[r] = ni;
         coeffs[j[k]] = nj;
-        if (a.rec_idx) record_pair(a, op, r, (u64)j[k], c[k], cj[k], to_j, to_i);
+        if (sm.rec_on) record_pair(a, sm, r, (u64)j[k], c[k], cj[k], to_j, to_i);
       }
     }
     unsigned masks[IT];
@@ -505,7 +507,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
       store_key<W>(keys, row, q);
       coeffs[row] = bval[k];
       set_row(a.table, slot[k], row);
-      if (a.rec_idx) a.rec_idx[a.rec_off[op] + (u64)t * TL + (u64)k * BLOCK + threadIdx.x] = (u32)row;
+      if (sm.rec_on) a.rec_idx[sm.rec_base + (u64)t * TL + (u64)k * BLOCK + threadIdx.x] = (u32)row;
     }
     __syncthreads();  // sm is reused by the next tile
   }
@@ -568,7 +570,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
           emit |= 1u << k;
           bval[k] = bi;
         }
-        if (a.rec_idx) record_single(a, op, r, c);
+        if (sm.rec_on) record_single(a, sm, r, c);
       } else {
         const double cj = __ldcg(coeffs + j);
         const double bj = __dmul_rn(__dmul_rn(cj, sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
@@ -581,7 +583,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
         if (to_j) nj = __dadd_rn(nj, bi);
         coeffs[r] = ni;
         coeffs[j] = nj;
-        if (a.rec_idx) record_pair(a, op, r, (u64)j, c, cj, to_j, to_i);
+        if (sm.rec_on) record_pair(a, sm, r, (u64)j, c, cj, to_j, to_i);
       }
     }
     unsigned masks[IT];
@@ -603,7 +605,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
       store_key<W>(keys, row, q);
       coeffs[row] = bval[k];
       insert<W>(q, row, a.table, a.table_mask, &st->error);
-      if (a.rec_idx) a.rec_idx[a.rec_off[op] + r] = (u32)row;
+      if (sm.rec_on) a.rec_idx[sm.rec_base + r] = (u32)row;
     }
     __syncthreads();
   }
@@ -692,6 +694,7 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
                      (j[3] < 0 || (u64)j[3] > r);
     u32 emit = 0;
     double bval[3] = {0.0, 0.0, 0.0};
+    u64 slot[3] = {NO_SLOT, NO_SLOT, NO_SLOT};
     if (own) {
       double c[4];
       bool p[4];
@@ -756,6 +759,9 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
         if (!born[m]) continue;
         emit |= 1u << (m - 1);
         bval[m - 1] = c[m];
+        u64 q[W];
+        member(m, q);
+        slot[m - 1] = claim_slot<W>(q, a.table, a.table_mask, &st->error);  // before the scan: see claim_slot
         if (born[m] == 1) {
           ++n_born1;
           if (a2) ++n_anti2;  // a row the first rotation creates here anticommutes with the second
@@ -777,7 +783,7 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
       member(k + 1, q);
       store_key<W>(keys, row, q);
       coeffs[row] = bval[k];
-      insert<W>(q, row, a.table, a.table_mask, &st->error);
+      set_row(a.table, slot[k], row);
     }
     __syncthreads();  // sm is reused by the next tile
   }
@@ -798,7 +804,7 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
 // (partitioned_termsum.rs:303-308, termsum.rs:551-557).
 template <int W, int ALG>
 __device__ __noinline__ void phase_op(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, const u64* keys,
-                                      double* coeffs, const Grp grp) {
+                                      double* coeffs, const TileSmem& sm, const Grp grp) {
   using Ops = typename Alg<ALG>::T;
   for (u64 r = (u64)grp.bid * BLOCK + threadIdx.x; r < N; r += (u64)grp.nblk * BLOCK) {
     u64 key[W];
@@ -806,7 +812,7 @@ __device__ __noinline__ void phase_op(const SweepArgs& a, const GateDesc<W>& d, 
     if (Ops::template anticommutes<W>(d.g, key)) {
       const double c = __ldcg(coeffs + r);
       coeffs[r] = __dmul_rn(c, d.cs);
-      if (a.rec_idx) a.rec_coef[a.rec_off[op] + r] = c;
+      if (sm.rec_on) a.rec_coef[sm.rec_base + r] = c;
     }
   }
 }
@@ -871,9 +877,9 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
                                         (!a.has_min_coeff || fabs(c) >= a.min_coeff);
       keep |= (u32)kp << k;
       if (kp) slot[k] = claim_slot<W>(key[k], a.table, a.table_mask, &st->error);
-      if (a.rec_idx) {
-        a.rec_idx[a.rec_off[op] + r] = REC_NONE;
-        store_key<W>(a.rec_keys + a.rec_key_off[op] * W, r, key[k]);
+      if (sm.rec_on) {
+        a.rec_idx[sm.rec_base + r] = REC_NONE;
+        store_key<W>(a.rec_keys + sm.rec_key_base * W, r, key[k]);
       }
     }
     unsigned masks[IT];
@@ -886,7 +892,7 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
       store_key<W>(keys_out, row, key[k]);
       coeffs_out[row] = cv[k];
       set_row(a.table, slot[k], row);
-      if (a.rec_idx) a.rec_idx[a.rec_off[op] + (u64)t * TL + (u64)k * BLOCK + threadIdx.x] = (u32)row;
+      if (sm.rec_on) a.rec_idx[sm.rec_base + (u64)t * TL + (u64)k * BLOCK + threadIdx.x] = (u32)row;
     }
     __syncthreads();
   }
@@ -918,7 +924,12 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   if (threadIdx.x == 0) {
     fetch_op(op);
     os.n = ld_volatile(&st->n[par]);
+    sm.rec_on = 0;
   }
+  // Adjoint recording: every block places the ops identically from the same
+  // live counts, so the offsets agree without communication.
+  u64 rb = a.rec_idx ? ld_volatile(&st->rec_next) : 0, rkb = a.rec_idx ? ld_volatile(&st->rec_key_next) : 0;
+  bool rec_on = a.rec_idx && !*(volatile u32*)&st->rec_full;
   __syncthreads();
   bool stopped = false;  // a capacity stop inside a fused op
   while (op < a.op_end) {
@@ -932,15 +943,36 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     u64* n_out = &st->n[par ^ 1u];
     const u32 nops = fused_count(od.kind);
     bool split = false;  // a fused op that ran its rotations one after the other
-    if (od.kind != OP_NOISE_SCALE && od.kind != OP_NOISE_COMPACT) {
-      if (2 * N > a.cap) {  // uniform: every block reads the same N
-        if (grp.bid == 0 && threadIdx.x == 0) st->halt = op;
-        break;
+    const bool gate_like = od.kind != OP_NOISE_SCALE && od.kind != OP_NOISE_COMPACT;
+    if (gate_like && 2 * N > a.cap) {  // uniform: every block reads the same N
+      if (grp.bid == 0 && threadIdx.x == 0) st->halt = op;
+      break;
+    }
+    if (a.rec_idx) {
+      const bool rec_op = gate_like || od.kind == OP_NOISE_COMPACT;
+      if (rec_on && rec_op &&
+          (rb + N > a.rec_cap || (od.kind == OP_NOISE_COMPACT && rkb + N > a.rec_key_cap)))
+        rec_on = false;  // the pool is full: this op and every later one go unrecorded
+      if (threadIdx.x == 0) {
+        sm.rec_on = rec_on && rec_op;
+        sm.rec_base = rb;
+        sm.rec_key_base = rkb;
+        if (grp.bid == 0) {
+          a.rec_off[op] = rb;
+          a.rec_key_off[op] = rkb;
+        }
       }
+      __syncthreads();
+      if (rec_on && rec_op) {
+        rb += N;
+        if (od.kind == OP_NOISE_COMPACT) rkb += N;
+      }
+    }
+    if (gate_like) {
       if (od.kind == OP_GATE) {
         gate_op<W, ALG>(a, sgs[0], op, N, keys, coeffs, sm, grp, n_out);
       } else if (od.kind == OP_PHASE) {
-        phase_op<W, ALG>(a, sgs[0], op, N, keys, coeffs, grp);
+        phase_op<W, ALG>(a, sgs[0], op, N, keys, coeffs, sm, grp);
         if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, N);
       } else if (N == 0) {
         if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
@@ -1019,6 +1051,11 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   if (grp.bid == 0 && threadIdx.x == 0) {
     st->cur = (u32)cur;
     st->end_op = op;
+    if (a.rec_idx) {
+      st->rec_next = rb;
+      st->rec_key_next = rkb;
+      st->rec_full = rec_on ? 0u : 1u;
+    }
     // The host reads the live count at n[end_op & 1].
     if ((op & 1u) != par) st->n[op & 1u] = ld_volatile(&st->n[par]);
     if (a.idle_blocks) atomicAdd(a.idle_blocks, grp.nblk);

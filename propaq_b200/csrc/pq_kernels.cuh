@@ -40,6 +40,9 @@ struct SweepState {
   u64 n[2];       // live rows: op k reads n[k & 1], writes n[(k + 1) & 1]
   u64 peak;       // largest live count the sweeps have seen
   u64 n_mid[2];   // live rows between the rotations of a fused op run one after the other
+  u64 rec_next;   // adjoint recording: next free element of rec_idx / rec_coef
+  u64 rec_key_next;  // ... next free key row of rec_keys
+  u32 rec_full;   // ... the pool ran out: no op from here on is recorded
   u32 halt;       // op at which a sweep stopped for capacity, or NOT_HALTED
   u32 error;      // ERR_* bits
   u32 cur;        // row buffer holding the live rows when the sweep ended
@@ -85,12 +88,16 @@ struct SweepArgs {
   // gate / phase ops store each anticommuting pre-op row's coefficient
   // (rec_coef) and the post-op row its sin branch went to, or REC_NONE
   // (rec_idx); a reclaim stores each row's new index or REC_NONE (rec_idx)
-  // and its pre-op keys from row rec_key_off[op] of rec_keys.
+  // and its pre-op keys from row rec_key_off[op] of rec_keys.  The sweep
+  // places the ops one after another from SweepState::rec_next /
+  // rec_key_next, writes rec_off / rec_key_off, and stops recording (sets
+  // rec_full) when the next op would not fit in rec_cap / rec_key_cap.
   u32* rec_idx;
   double* rec_coef;
   u64* rec_keys;
-  const u64* rec_off;
-  const u64* rec_key_off;
+  u64* rec_off;
+  u64* rec_key_off;
+  u64 rec_cap, rec_key_cap;
   // Decisions made on the host for a launch of one op (null: the device's own
   // rules).  host_state: per input row, the emit state of its sin branch
   // (S_EMIT 0 / S_HELD 1), from a truncator plugin's keep.  host_factor: per

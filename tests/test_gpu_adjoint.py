@@ -26,11 +26,19 @@ from propaq_b200.adjoint import ParametrizedExpectation, _heisenberg_order
 pytestmark = pytest.mark.gpu
 
 
-def gpu_grad(engine, p, checkpoint_layers=0):
+def gpu_grad(engine, p, checkpoint_layers=0, record_bytes=0):
     cfg, keep = make_cfg(p, want_terms=False)
     res, nt, g = engine.run_adjoint(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag,
-                                    checkpoint_layers=checkpoint_layers)
+                                    checkpoint_layers=checkpoint_layers, record_bytes=record_bytes)
     return res, nt, g
+
+
+def replay_pool(p, nt):
+    """A record pool too small for the whole run but large enough for any one
+    layer's ops: the gradient then re-runs layer segments to record them."""
+    n_in = np.concatenate([[len(p.obs_coeffs)], nt[:-1]]).astype(float)
+    total = 12 * n_in.sum() + 64 * n_in.sum() / 4  # rotations, plus room for reclaim snapshots
+    return int(0.6 * total)
 
 
 @pytest.mark.parametrize("seed", range(4))
@@ -74,10 +82,28 @@ def test_gradient_matches_forward_mode_reference(gpu_engine, oracle, case, seed)
         L = len(p.offsets) - 1
         p.noise_tables_layered = np.array([[math.exp(-0.01 * (l + 1) * w) for w in range(n + 1)] for l in range(L)])
     e_ref, g_ref = propagate_with_tangents(oracle, p)
-    res, _, g = gpu_grad(gpu_engine, p, checkpoint_layers=3)
+    res, nt, g = gpu_grad(gpu_engine, p, checkpoint_layers=3)
     assert abs(res.expectation_value - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
     scale = max(1.0, float(np.abs(g_ref).max()))
     np.testing.assert_allclose(g, g_ref, rtol=1e-9, atol=1e-12 * scale)
+    _, _, g2 = gpu_grad(gpu_engine, p, checkpoint_layers=1, record_bytes=replay_pool(p, nt))
+    np.testing.assert_allclose(g2, g_ref, rtol=1e-9, atol=1e-12 * scale)
+
+
+@pytest.mark.parametrize("wl", [workloads.hardware_efficient(12, 5, seed=2), workloads.kicked_ising(4, 5, 4)],
+                         ids=["hea", "kicked_noisy"])
+def test_recording_in_the_forward_pass_equals_replayed_segments(gpu_engine, wl):
+    # One reverse sweep over records made in the forward pass, and segment
+    # replays into a small pool, give the same gradient bit for bit.
+    p = from_workload(wl)
+    full = gpu_grad(gpu_engine, p, 1)
+    replayed = gpu_grad(gpu_engine, p, 1, record_bytes=replay_pool(p, full[1]))
+    assert replayed[0].gpu_launches > full[0].gpu_launches, "the small pool must force replays"
+    ok = ~np.isnan(full[2])
+    assert np.array_equal(np.isnan(replayed[2]), ~ok)
+    assert np.array_equal(replayed[2][ok], full[2][ok])
+    with pytest.raises(MemoryError, match="fewer checkpoint layers"):
+        gpu_grad(gpu_engine, p, 0, record_bytes=1 << 12)
 
 
 def test_checkpoint_segments_do_not_change_the_gradient(gpu_engine):
