@@ -33,12 +33,16 @@ def gpu_grad(engine, p, checkpoint_layers=0, record_bytes=0):
     return res, nt, g
 
 
-def replay_pool(p, nt):
-    """A record pool too small for the whole run but large enough for any one
-    layer's ops: the gradient then re-runs layer segments to record them."""
-    n_in = np.concatenate([[len(p.obs_coeffs)], nt[:-1]]).astype(float)
-    total = 12 * n_in.sum() + 64 * n_in.sum() / 4  # rotations, plus room for reclaim snapshots
-    return int(0.6 * total)
+def replay_pool(p, res):
+    """A record pool 2% short of what the whole run records, so the gradient
+    re-runs segments to record them (one at a time, each well inside the
+    pool).  The forward run records one 12-byte element per row entering each
+    rotation or reclaim, and one key per row entering each reclaim; the pool
+    gives 85% of its bytes to the elements and 15% to the keys."""
+    reclaim = p.max_weight is not None or p.min_coeff is not None or p.min_terms is not None
+    keys = res.sum_rows_noise if reclaim else 0
+    rows = res.sum_rows_gate + res.sum_rows_phase + keys
+    return int(max(0.98 * rows * 12 / 0.85, 0.98 * keys * 8 * p.n_words / 0.15))
 
 
 @pytest.mark.parametrize("seed", range(4))
@@ -86,7 +90,7 @@ def test_gradient_matches_forward_mode_reference(gpu_engine, oracle, case, seed)
     assert abs(res.expectation_value - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
     scale = max(1.0, float(np.abs(g_ref).max()))
     np.testing.assert_allclose(g, g_ref, rtol=1e-9, atol=1e-12 * scale)
-    _, _, g2 = gpu_grad(gpu_engine, p, checkpoint_layers=1, record_bytes=replay_pool(p, nt))
+    _, _, g2 = gpu_grad(gpu_engine, p, checkpoint_layers=1, record_bytes=replay_pool(p, res))
     np.testing.assert_allclose(g2, g_ref, rtol=1e-9, atol=1e-12 * scale)
 
 
@@ -96,8 +100,9 @@ def test_recording_in_the_forward_pass_equals_replayed_segments(gpu_engine, wl):
     # One reverse sweep over records made in the forward pass, and segment
     # replays into a small pool, give the same gradient bit for bit.
     p = from_workload(wl)
+    gpu_grad(gpu_engine, p, 1)  # the engine's buffers grow to size here
     full = gpu_grad(gpu_engine, p, 1)
-    replayed = gpu_grad(gpu_engine, p, 1, record_bytes=replay_pool(p, full[1]))
+    replayed = gpu_grad(gpu_engine, p, 1, record_bytes=replay_pool(p, full[0]))
     assert replayed[0].gpu_launches > full[0].gpu_launches, "the small pool must force replays"
     ok = ~np.isnan(full[2])
     assert np.array_equal(np.isnan(replayed[2]), ~ok)
