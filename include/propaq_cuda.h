@@ -202,9 +202,12 @@ int pq_run_batch(pq_engine* engine, const pq_instance* instances, size_t n, cons
  * it backs a torch.autograd.Function over the propagators.
  *
  * Arguments as pq_run; diag_state is required.  The forward run records what
- * the reverse pass needs into a pool of record_bytes of device memory (0 =
- * 40% of the free memory, at most 48 GB): 12 bytes per row entering each
- * rotation.  When it all fits, one reverse sweep follows.  Otherwise the
+ * the reverse pass needs into a pool of record_bytes of device memory: 12
+ * bytes per row entering each rotation.  0 = the size the engine's last
+ * default-sized gradient needed plus a quarter (at first 40% of the free
+ * memory, at most 48 GB); the engine keeps the pool, the adjoint vectors and
+ * the checkpoints between calls and frees them in pq_engine_destroy.  When it
+ * all fits, one reverse sweep follows.  Otherwise the
  * forward run's terms at the start of every checkpoint_layers layers (0 = one
  * segment) are used to re-run one segment at a time while recording.  Gates
  * deferred into the Clifford frame (fixed Clifford rotations) get NaN.  A

@@ -20,7 +20,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libpropaq_cuda.so"
 SOURCES = ["pq_kernels.cu", "pq_host.cu", "pq_noalloc.cu"]
-HEADERS = ["pq_device.cuh", "pq_kernels.cuh"]
+HEADERS = ["pq_device.cuh", "pq_kernels.cuh", "pq_tableau.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -33,9 +33,17 @@
 
 #include "../../include/propaq_cuda.h"
 #include "pq_kernels.cuh"
+#include "pq_tableau.h"
 
 using pq::u32;
 using pq::u64;
+using pqh::EVEN;
+using pqh::hpopc;
+using pqh::host_anticommutes;
+using pqh::host_product_exp;
+using pqh::host_support;
+using pqh::host_weight;
+using pqh::Tableau;
 
 namespace {
 
@@ -43,203 +51,6 @@ constexpr double EPS_CLASSIFY = 1e-9;  // termsum.rs:42, partitioned_termsum.rs:
 constexpr u32 MAX_UNITS = 2048;        // engine.rs:27
 constexpr u64 MAX_ROWS = 1ULL << 31;   // row index ceiling of the table slots
 constexpr int TILE_ROWS = 256;  // smallest tile a sweep uses (sizes the look-back status array)
-
-inline int hpopc(u64 x) { return __builtin_popcountll(x); }
-constexpr u64 EVEN = 0x5555555555555555ULL;
-
-// ------------------------------------------------------------ host algebra
-// Phase exponent p of G*K = i^p (G xor K); the same formulas as the device
-// (crates/pauli/src/algebra.rs:206-213, crates/majorana/src/algebra.rs:180-193).
-int host_product_exp(int alg, int W, const u64* g, const u64* k) {
-  if (alg == 0) {
-    int yg = 0, yk = 0, yo = 0, zx = 0;
-    for (int i = 0; i < W; ++i) {
-      u64 o = k[i] ^ g[i];
-      yg += hpopc(g[i] & (g[i] >> 1) & EVEN);
-      yk += hpopc(k[i] & (k[i] >> 1) & EVEN);
-      yo += hpopc(o & (o >> 1) & EVEN);
-      zx += hpopc((g[i] >> 1) & k[i] & EVEN);
-    }
-    return (yg + yk - yo + 2 * zx) & 3;
-  }
-  int lg = 0, lk = 0, lo = 0, sw = 0;
-  int above = 0;
-  for (int i = W - 1; i >= 0; --i) {
-    u64 o = k[i] ^ g[i];
-    int pg = hpopc(g[i]), pk = hpopc(k[i]);
-    lg += pg;
-    lk += pk;
-    lo += hpopc(o);
-    u64 s = g[i] >> 1;
-    for (int sh = 1; sh < 64; sh <<= 1) s ^= s >> sh;
-    sw ^= (hpopc(k[i] & s) & 1) ^ (pk & above);
-    above ^= pg & 1;
-  }
-  auto herm = [](int l) { return ((l & 3) >= 2) ? 1 : 0; };
-  return (herm(lg) + herm(lk) - herm(lo) + 2 * (sw & 1)) & 3;
-}
-bool host_anticommutes(int alg, int W, const u64* g, const u64* k) {
-  if (alg == 0) {
-    u64 acc = 0;
-    for (int i = 0; i < W; ++i) acc ^= k[i] & (((g[i] & EVEN) << 1) | ((g[i] >> 1) & EVEN));
-    return hpopc(acc) & 1;
-  }
-  int ov = 0, lg = 0, lk = 0;
-  for (int i = 0; i < W; ++i) {
-    ov += hpopc(k[i] & g[i]);
-    lg += hpopc(g[i]);
-    lk += hpopc(k[i]);
-  }
-  return ((ov + ((lg & 1) ? lk : 0)) & 1) == 1;
-}
-int host_support(int W, const u64* k) {
-  int n = 0;
-  for (int i = 0; i < W; ++i) n += hpopc((k[i] | (k[i] >> 1)) & EVEN);
-  return n;
-}
-u32 host_weight(int alg, int W, const u64* k, u32 n_units) {
-  if (alg == 0) return (u32)host_support(W, k);
-  int total = 0;
-  for (int i = 0; i < W; ++i) total += hpopc((k[i] ^ (k[i] >> 1)) & EVEN);
-  bool odd = total & 1;
-  u32 w = 0;
-  u64 carry = 0;
-  for (int i = 0; i < W; ++i) {
-    u64 s = (k[i] ^ (k[i] >> 1)) & EVEN, occ = (k[i] | (k[i] >> 1)) & EVEN, p = s;
-    for (int sh = 2; sh < 64; sh <<= 1) p ^= p << sh;
-    p ^= carry;
-    carry = (p >> 62) & 1 ? EVEN : 0;
-    long live_sites = (long)n_units - (long)i * 32;
-    u64 live = live_sites <= 0 ? 0 : (live_sites >= 32 ? EVEN : (EVEN & ((1ULL << (2 * live_sites)) - 1)));
-    u64 str = (odd ? (p ^ EVEN) : p) & live;
-    w += hpopc((s | (occ ^ str)) & live);
-  }
-  return w;
-}
-
-// --------------------------------------------------------------- tableau
-// A deferred Clifford frame (crates/core/src/algebra/tableau.rs:29-223):
-// 2n rows, a readout map P -> C^dag P C and its inverse generator map.
-struct Tableau {
-  int alg = 0, W = 1;
-  size_t rows = 0;
-  std::vector<u64> rd_img, gen_img;  // rows x W
-  std::vector<int> rd_sign, gen_sign;
-  bool identity = true;
-
-  Tableau() = default;
-  Tableau(int a, int w, u32 n_units) : alg(a), W(w), rows(2 * (size_t)n_units) {
-    rd_img.assign(rows * W, 0);
-    rd_sign.assign(rows, 1);
-    for (size_t p = 0; p < rows; ++p)
-      if (p < (size_t)64 * W) rd_img[p * W + p / 64] = 1ULL << (p % 64);
-    gen_img = rd_img;
-    gen_sign = rd_sign;
-  }
-  bool row_is_unit(const std::vector<u64>& img, size_t p) const {
-    for (int i = 0; i < W; ++i) {
-      u64 want = (p < (size_t)64 * W && (size_t)i == p / 64) ? (1ULL << (p % 64)) : 0;
-      if (img[p * W + i] != want) return false;
-    }
-    return true;
-  }
-  void refresh_identity() {
-    identity = true;
-    for (size_t p = 0; p < rows && identity; ++p)
-      if (!row_is_unit(rd_img, p) || rd_sign[p] != 1) identity = false;
-  }
-  // apply_rows (tableau.rs:109-143) with phases as exponents of i.
-  int apply(const std::vector<u64>& img, const std::vector<int>& sgn, const u64* mono, u64* out) const {
-    std::vector<u64> src(W, 0), e(W, 0), g(W);
-    for (int i = 0; i < W; ++i) out[i] = 0;
-    int se = 0, ie = 0;
-    for (int wi = 0; wi < W; ++wi) {
-      u64 bits = mono[wi];
-      while (bits) {
-        int b = __builtin_ctzll(bits);
-        bits &= bits - 1;
-        size_t p = (size_t)wi * 64 + b;
-        if (p >= rows) continue;
-        std::fill(e.begin(), e.end(), 0);
-        e[wi] = 1ULL << b;
-        se += host_product_exp(alg, W, e.data(), src.data());
-        src[wi] ^= e[wi];
-        for (int i = 0; i < W; ++i) g[i] = img[p * W + i];
-        ie += host_product_exp(alg, W, g.data(), out) + (sgn[p] < 0 ? 2 : 0);
-        for (int i = 0; i < W; ++i) out[i] ^= g[i];
-      }
-    }
-    return (((ie - se) & 3) == 2) ? -1 : 1;
-  }
-  int conjugate_generator(const u64* mono, u64* out) const {
-    if (identity) {
-      std::memcpy(out, mono, 8 * W);
-      return 1;
-    }
-    return apply(gen_img, gen_sign, mono, out);
-  }
-  void compose(const Tableau& next) {
-    if (next.identity) return;
-    std::vector<u64> r2(rows * W), g2(next.rows * W);
-    std::vector<int> rs(rows), gs(next.rows);
-    for (size_t i = 0; i < rows; ++i) rs[i] = next.apply(next.rd_img, next.rd_sign, &rd_img[i * W], &r2[i * W]) * rd_sign[i];
-    for (size_t i = 0; i < next.rows; ++i)
-      gs[i] = apply(gen_img, gen_sign, &next.gen_img[i * W], &g2[i * W]) * next.gen_sign[i];
-    rd_img.swap(r2);
-    rd_sign.swap(rs);
-    gen_img.swap(g2);
-    gen_sign.swap(gs);
-    refresh_identity();
-  }
-  // for_rotation (tableau.rs:180-209), for |cos(angle)| < eps.
-  static Tableau for_rotation(int alg, int W, u32 n_units, const u64* gen, double angle) {
-    Tableau t(alg, W, n_units);
-    const double sn = std::sin(angle);
-    size_t lim = std::min(t.rows, (size_t)64 * W);
-    std::vector<u64> e(W), img(W);
-    for (size_t p = 0; p < lim; ++p) {
-      std::fill(e.begin(), e.end(), 0);
-      e[p / 64] = 1ULL << (p % 64);
-      if (!host_anticommutes(alg, W, gen, e.data())) continue;
-      int pe = host_product_exp(alg, W, gen, e.data());
-      for (int i = 0; i < W; ++i) img[i] = gen[i] ^ e[i];
-      // sign = sin * (-Im i^p); the rotation is Clifford so |sin| rounds to 1.
-      double nim = pe == 1 ? -1.0 : (pe == 3 ? 1.0 : 0.0);
-      double sign = sn * nim;
-      int s = sign < 0 ? -1 : 1;
-      for (int i = 0; i < W; ++i) t.rd_img[p * W + i] = t.gen_img[p * W + i] = img[i];
-      t.rd_sign[p] = s;
-      t.gen_sign[p] = -s;
-    }
-    t.refresh_identity();
-    return t;
-  }
-  // changes_weight of for_rotation(gen) without building the tableau: a
-  // single-bit row keeps its image unless it anticommutes with gen, and then
-  // its image is gen ^ e_p.
-  static bool rotation_changes_weight(int alg, int W, u32 n_units, const u64* gen) {
-    const size_t lim = std::min((size_t)2 * n_units, (size_t)64 * W);
-    u64 e[64] = {0}, img[64];
-    for (size_t p = 0; p < lim; ++p) {
-      e[p / 64] = 1ULL << (p % 64);
-      const bool anti = host_anticommutes(alg, W, gen, e);
-      e[p / 64] = 0;
-      if (!anti) continue;
-      for (int i = 0; i < W; ++i) img[i] = gen[i];
-      img[p / 64] ^= 1ULL << (p % 64);
-      if (host_support(W, img) != 1) return true;
-    }
-    return false;
-  }
-  bool changes_weight() const {
-    for (size_t p = 0; p < rows; ++p) {
-      std::vector<u64> u(W, 0);
-      if (p < (size_t)64 * W) u[p / 64] = 1ULL << (p % 64);
-      if (host_support(W, &rd_img[p * W]) != host_support(W, u.data())) return true;
-    }
-    return false;
-  }
-};
 
 // --------------------------------------------------------------- plugins
 struct Plugin {
@@ -432,6 +243,34 @@ cudaError_t grow_pair(T** dev, T** host, size_t* cap, size_t n) {
 
 }  // namespace
 
+// A grow-only device buffer the engine keeps between calls, carved into
+// typed arrays by byte offset.  Released by the engine.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t n) {
+    if (bytes >= n) return cudaSuccess;
+    release();
+    const cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    bytes = n;
+    return cudaSuccess;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* at(size_t offset) const {
+    return reinterpret_cast<T*>(static_cast<char*>(p) + offset);
+  }
+};
+inline size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
 struct pq_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -451,6 +290,13 @@ struct pq_engine {
   u32* d_err = nullptr;   // error word of the stand-alone kernels
   u32* d_idle = nullptr;  // blocks left idle in a batched launch
   u64 launches = 0;
+  // Gradient buffers (pq_run_adjoint), kept so that repeated gradients of
+  // one problem allocate nothing: the record pool, the two adjoint vectors
+  // and per-op arrays, the segment checkpoints, and the pool size the last
+  // default-sized gradient needed to record every op.
+  DevBuf g_pool, g_lam, g_ops;
+  std::vector<DevBuf> g_ck;
+  size_t g_need = 0;
 
   int fail(int code, const std::string& m) {
     err = m;
@@ -464,6 +310,8 @@ struct pq_engine {
   ~pq_engine() {
     if (stream) cudaStreamSynchronize(stream);
     for (auto& s : slots) s.free_all();
+    for (DevBuf* b : {&g_pool, &g_lam, &g_ops}) b->release();
+    for (DevBuf& b : g_ck) b.release();
     for (void* p : {(void*)d_states, (void*)d_args, (void*)d_block_inst, (void*)d_err, (void*)d_idle})
       if (p) cudaFree(p);
     for (void* p : {(void*)h_states, (void*)h_args, (void*)h_block_inst})
@@ -818,7 +666,7 @@ int build_ops(Plan& P, NeedN need_n) {
           if (n < P.floor_terms) eff_w = false;
         }
         if (!eff_w || !cw) {
-          P.frame.compose(Tableau::for_rotation(ALG, W, P.n_units, g.data(), ang));
+          P.frame.compose_rotation(g.data(), ang);
           P.gate_op[gi] = P.last_op;
           continue;
         }
@@ -1395,25 +1243,12 @@ int run_one(pq_engine* E, const Inputs& in, int W) {
 }
 
 // Device buffers of one adjoint run, freed on every exit path.
-struct RunBuffers {
-  std::vector<void*> ptrs;
-  ~RunBuffers() {
-    for (void* p : ptrs) cudaFree(p);
-  }
-  template <class T>
-  cudaError_t alloc(T** p, size_t n) {
-    *p = nullptr;
-    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T));
-    if (e == cudaSuccess) ptrs.push_back(*p);
-    return e;
-  }
-};
-
 // Expectation value and dE/d(angle) of every gate with the truncation
 // decisions of the forward run held fixed.  The forward run records each op
 // (SweepArgs::rec_idx: sin-branch partners, pre-op coefficients, reclaim maps
-// and key snapshots) into a pool of record_bytes (0: 40% of the free device
-// memory, at most 48 GB) and keeps the live terms at the start of every
+// and key snapshots) into a pool of record_bytes (0: what the last such
+// gradient needed plus a quarter, at first 40% of the free device memory, at
+// most 48 GB; the engine keeps the pool) and keeps the live terms at the start of every
 // segment of ckpt_layers layers.  If every op fit, one reverse sweep
 // (adjoint_kernel) carries dE/dc from the final rows back to the observable.
 // If the pool ran out, the reverse pass goes segment by segment, last first:
@@ -1450,35 +1285,49 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, u64 reco
   for (size_t l = 0; l < in.n_layers; l += per) seg.push_back(P.layer_op[l]);
   seg.push_back(n_ops);
   const size_t n_seg = seg.size() - 1;
-  RunBuffers mem;
   cudaError_t e;
 
-  // The record pool: a share of the free device memory, split between the
-  // per-row records (12 B an element) and reclaim key snapshots.
+  // The record pool, split between the per-row records (12 B an element) and
+  // reclaim key snapshots: record_bytes, else the size the last default-sized
+  // gradient needed (plus a quarter), else 40% of the free device memory (at
+  // most 48 GB).  The engine keeps it for the next gradient.
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
-  const size_t budget = record_bytes ? (size_t)record_bytes : std::min<size_t>(free_b / 5 * 2, (size_t)48 << 30);
+  const size_t ceiling = std::min<size_t>((free_b + E->g_pool.bytes) / 5 * 2, (size_t)48 << 30);
   Recording rec;
-  rec.cap = std::max<u64>(budget / 100 * 85 / 12, 1);
-  rec.key_cap = std::max<u64>(budget / 100 * 15 / (8 * (size_t)W), 1);
-  if ((e = mem.alloc(&rec.idx, rec.cap)) != cudaSuccess || (e = mem.alloc(&rec.coef, rec.cap)) != cudaSuccess ||
-      (e = mem.alloc(&rec.keys, rec.key_cap * W)) != cudaSuccess || (e = mem.alloc(&rec.off, n_ops)) != cudaSuccess ||
-      (e = mem.alloc(&rec.key_off, n_ops)) != cudaSuccess)
-    return E->cuda_fail(e, "gradient record pool");
+  auto setup_pool = [&](size_t budget) -> cudaError_t {
+    rec.cap = std::max<u64>(budget / 100 * 85 / 12, 1);
+    rec.key_cap = std::max<u64>(budget / 100 * 15 / (8 * (size_t)W), 1);
+    const size_t o_coef = align256(4 * rec.cap), o_keys = o_coef + align256(8 * rec.cap),
+                 o_off = o_keys + align256(8 * (size_t)W * rec.key_cap), o_koff = o_off + align256(8 * n_ops),
+                 pool_end = o_koff + align256(8 * n_ops);
+    if (E->g_pool.bytes < pool_end) E->g_pool.release();  // before the new one, so both never coexist
+    if (cudaError_t ee = E->g_pool.ensure(pool_end)) return ee;
+    rec.idx = E->g_pool.at<u32>(0);
+    rec.coef = E->g_pool.at<double>(o_coef);
+    rec.keys = E->g_pool.at<u64>(o_keys);
+    rec.off = E->g_pool.at<u64>(o_off);
+    rec.key_off = E->g_pool.at<u64>(o_koff);
+    return cudaSuccess;
+  };
+  size_t budget = record_bytes ? (size_t)record_bytes : (E->g_need ? std::min(E->g_need / 4 * 5, ceiling) : ceiling);
+  if ((e = setup_pool(budget)) != cudaSuccess) return E->cuda_fail(e, "gradient record pool");
 
   // Forward, keeping each segment's starting terms and recording every op
   // while the pool lasts.
   std::vector<u64*> ck_keys(n_seg, nullptr);
   std::vector<double*> ck_coeffs(n_seg, nullptr);
   std::vector<u64> ck_n(n_seg, 0);
+  if (E->g_ck.size() < n_seg) E->g_ck.resize(n_seg);
   bool began = false;
   P.rec_next = P.rec_key_next = 0;
   P.rec_full = 0;
   for (size_t s = 0; s < n_seg; ++s) {
     ck_n[s] = P.n_live;
-    if ((e = mem.alloc(&ck_keys[s], ck_n[s] * W)) != cudaSuccess ||
-        (e = mem.alloc(&ck_coeffs[s], ck_n[s])) != cudaSuccess)
-      return E->cuda_fail(e, "checkpoint");
+    const size_t o_c = align256(8 * (size_t)W * ck_n[s]);
+    if ((e = E->g_ck[s].ensure(o_c + 8 * ck_n[s])) != cudaSuccess) return E->cuda_fail(e, "checkpoint");
+    ck_keys[s] = E->g_ck[s].at<u64>(0);
+    ck_coeffs[s] = E->g_ck[s].at<double>(o_c);
     cudaMemcpyAsync(ck_keys[s], S.keys[S.cur], ck_n[s] * W * 8, cudaMemcpyDeviceToDevice, E->stream);
     cudaMemcpyAsync(ck_coeffs[s], S.coeffs[S.cur], ck_n[s] * 8, cudaMemcpyDeviceToDevice, E->stream);
     if (int rc = execute_single(E, S, P, grid, &began, seg[s + 1], &rec)) return rc;
@@ -1495,6 +1344,22 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, u64 reco
   std::vector<u64> hist(n_ops), n_in(n_ops), koff(n_ops, 0);
   if (n_ops) cudaMemcpy(hist.data(), S.hist, n_ops * 8, cudaMemcpyDeviceToHost);
   for (size_t k = 0; k < n_ops; ++k) n_in[k] = k ? hist[k - 1] : P.n0;
+  if (!record_bytes) {  // the pool that records every op of this run
+    u64 rows = 0, keys = 0;
+    for (size_t k = 0; k < n_ops; ++k) {
+      if (P.ops[k].kind == pq::OP_NOISE_SCALE) continue;
+      rows += n_in[k];
+      if (P.ops[k].kind == pq::OP_NOISE_COMPACT) keys += n_in[k];
+    }
+    E->g_need = std::max<size_t>(rows * 12 / 85 * 100 + 100, keys * 8 * (size_t)W / 15 * 100 + 100);
+    // A default pool sized for an earlier, smaller problem: grow it to this
+    // run's need before the segments are re-run to record them.
+    const size_t want = std::min(E->g_need / 4 * 5, ceiling);
+    if (!recorded_all && want > budget) {
+      budget = want;
+      if ((e = setup_pool(budget)) != cudaSuccess) return E->cuda_fail(e, "gradient record pool");
+    }
+  }
   std::vector<long long> gate_ops(in.n_gates);
   for (size_t g = 0; g < in.n_gates; ++g) gate_ops[g] = P.gate_own[g] ? P.gate_op[g] : -1;
   double* lam[2] = {nullptr, nullptr};
@@ -1503,11 +1368,20 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, u64 reco
   u64* d_n_in = nullptr;
   long long* d_gate_ops = nullptr;
   const u64** d_ksrc = nullptr;
-  if ((e = mem.alloc(&lam[0], S.cap)) != cudaSuccess || (e = mem.alloc(&lam[1], S.cap)) != cudaSuccess ||
-      (e = mem.alloc(&grad_part, n_ops * (size_t)agrid)) != cudaSuccess ||
-      (e = mem.alloc(&d_grad, in.n_gates)) != cudaSuccess || (e = mem.alloc(&d_n_in, n_ops)) != cudaSuccess ||
-      (e = mem.alloc(&d_gate_ops, in.n_gates)) != cudaSuccess || (e = mem.alloc(&d_ksrc, n_ops)) != cudaSuccess)
-    return E->cuda_fail(e, "adjoint buffers");
+  if ((e = E->g_lam.ensure(align256(8 * S.cap) * 2)) != cudaSuccess) return E->cuda_fail(e, "adjoint vectors");
+  lam[0] = E->g_lam.at<double>(0);
+  lam[1] = E->g_lam.at<double>(align256(8 * S.cap));
+  {
+    const size_t o_grad = align256(8 * n_ops * (size_t)agrid), o_nin = o_grad + align256(8 * in.n_gates),
+                 o_gops = o_nin + align256(8 * n_ops), o_ksrc = o_gops + align256(8 * in.n_gates),
+                 end = o_ksrc + align256(8 * n_ops);
+    if ((e = E->g_ops.ensure(end)) != cudaSuccess) return E->cuda_fail(e, "adjoint buffers");
+    grad_part = E->g_ops.at<double>(0);
+    d_grad = E->g_ops.at<double>(o_grad);
+    d_n_in = E->g_ops.at<u64>(o_nin);
+    d_gate_ops = E->g_ops.at<long long>(o_gops);
+    d_ksrc = E->g_ops.at<const u64*>(o_ksrc);
+  }
   if (n_ops) {
     cudaMemcpyAsync(d_n_in, n_in.data(), n_ops * 8, cudaMemcpyHostToDevice, E->stream);
     cudaMemsetAsync(grad_part, 0, n_ops * (size_t)agrid * 8, E->stream);
@@ -1611,6 +1485,9 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, u64 reco
   float ms = 0;
   cudaEventElapsedTime(&ms, E->ev_begin, E->ev_end);
   in.res->device_ms = ms;
+  // A default-sized pool far above what this run needed is given back; the
+  // next gradient allocates the measured size.
+  if (!record_bytes && E->g_pool.bytes / 2 > E->g_need / 4 * 5 + 32 * n_ops) E->g_pool.release();
   return PQ_OK;
 }
 

@@ -111,6 +111,24 @@ def test_recording_in_the_forward_pass_equals_replayed_segments(gpu_engine, wl):
         gpu_grad(gpu_engine, p, 0, record_bytes=1 << 12)
 
 
+def test_default_pool_follows_the_problem(gpu_engine):
+    # The engine keeps the default-sized pool at what the last gradient
+    # needed; a larger problem after a small one outgrows it, grows it and
+    # re-runs segments; the gradient is the same as with an explicit pool.
+    small = from_workload(workloads.hardware_efficient(6, 2, seed=1))
+    big = from_workload(workloads.hardware_efficient(12, 5, seed=2))
+    ref = gpu_grad(gpu_engine, big, 1, record_bytes=1 << 30)
+    gpu_grad(gpu_engine, small, 1)
+    after_small = gpu_grad(gpu_engine, big, 1)
+    again = gpu_grad(gpu_engine, big, 1)
+    assert after_small[0].gpu_launches > again[0].gpu_launches, "the first big gradient must re-run segments"
+    ok = ~np.isnan(ref[2])
+    for r in (after_small, again):
+        assert r[0].expectation_value == ref[0].expectation_value
+        assert np.array_equal(np.isnan(r[2]), ~ok)
+        assert np.array_equal(r[2][ok], ref[2][ok])
+
+
 def test_checkpoint_segments_do_not_change_the_gradient(gpu_engine):
     wl = workloads.hardware_efficient(12, 5, seed=2)
     p = from_workload(wl)
