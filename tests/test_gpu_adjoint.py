@@ -8,7 +8,10 @@
     derivatives through the same decisions;
   - checkpointing changes memory, not results: every segment length gives
     bit-identical gradients;
-  - the full config: central finite differences on 20 seeded angles.
+  - the full config: central finite differences on 20 seeded angles;
+  - the surrogate derivative: the reference's surrogate model of the same
+    circuit (restated in oracle/pq_surrogate.py), differentiated over its
+    tape, on the ansatz untruncated and on a weight-cut circuit.
 """
 
 import math
@@ -109,6 +112,36 @@ def test_recording_in_the_forward_pass_equals_replayed_segments(gpu_engine, wl):
     assert np.array_equal(replayed[2][ok], full[2][ok])
     with pytest.raises(MemoryError, match="fewer checkpoint layers"):
         gpu_grad(gpu_engine, p, 0, record_bytes=1 << 12)
+
+
+SURROGATE_CASES = [
+    # the gradient's ansatz (RY, RZ, CNOT ladder; sum Z_i Z_i+1; |0..0>), untruncated
+    (lambda: workloads.hardware_efficient(6, 3, seed=7, sigma=0.6, max_weight=None, min_coeff=None)),
+    (lambda: workloads.hardware_efficient(8, 4, seed=7, sigma=0.6, max_weight=None, min_coeff=None)),
+    # a weight cut with no Clifford rotation: the surrogate's post-gate cut and
+    # the engine's emit-time cut keep the same terms
+    (lambda: workloads.tfim_chain(16, 6, seed=3, max_weight=4, min_coeff=None)),
+]
+
+
+@pytest.mark.parametrize("make", SURROGATE_CASES, ids=["hea6x3", "hea8x4", "tfim16-w4"])
+def test_gradient_matches_the_surrogate_derivative(gpu_engine, make):
+    # The surrogate model's derivative (reverse mode over its tape, one
+    # parameter per rotation) against the adjoint gradient: the same function
+    # of the angles wherever the truncation is structural.
+    from surrogate_ref import build_surrogate
+
+    wl = make()
+    p = from_workload(wl)
+    res, _, g = gpu_grad(gpu_engine, p, 1)
+    model = build_surrogate(p, weight=wl.max_weight)
+    th = list(p.angles)
+    e_s, g_s = model.evaluate(th), np.array(model.gradient(th))
+    assert abs(res.expectation_value - e_s) <= 1e-10 * max(1.0, abs(e_s))
+    param = np.abs(np.cos(p.angles)) >= 1e-9  # the CNOT pieces are fixed rotations
+    assert np.array_equal(~np.isnan(g), param)
+    scale = max(1.0, float(np.abs(g_s).max()))
+    np.testing.assert_allclose(g[param], g_s[param], rtol=1e-9, atol=1e-12 * scale)
 
 
 def test_default_pool_follows_the_problem(gpu_engine):
