@@ -319,6 +319,91 @@ __device__ __forceinline__ long long lookup(const u64* q, u64 n_pre, const u64* 
   return lookup_from<W>(q, fp, (b + 4) & mask, n_pre, keys, table, mask, st);
 }
 
+// lookup for a gate's partner search.  On a fingerprint match the candidate
+// row's coefficient is loaded together with its key, so a found partner costs
+// one round trip less (cj receives it); on a miss, `empty` receives the empty
+// slot where the probe ended, which is the first slot an insert of q would
+// take (every slot before it on q's probe sequence is occupied, and occupied
+// slots stay occupied during an op), or NO_SLOT.
+template <int W>
+__device__ long long lookup_from_c(const u64* q, u32 fp, u64 i, u64 n_pre, const u64* keys, const double* coeffs,
+                                   const u64* table, u64 mask, SweepState* st, double& cj, u64& empty) {
+  for (u64 probe = 0; probe <= mask; ++probe) {
+    const u64 s = __ldcg(table + i);
+    if (s == EMPTY_SLOT) {
+      empty = i;
+      return -1;
+    }
+    const u32 row = (u32)s;
+    if ((u32)(s >> 32) == fp && row < n_pre) {
+      const u64* kp = keys + (u64)row * W;
+      const double c = __ldcg(coeffs + row);
+      bool eq = true;
+#pragma unroll
+      for (int w = 0; w < W; ++w) eq &= __ldcg(kp + w) == q[w];
+      if (eq) {
+        cj = c;
+        return row;
+      }
+    }
+    i = (i + 1) & mask;
+  }
+  atomicOr(&st->error, ERR_PROBE_OVERFLOW);
+  empty = NO_SLOT;
+  return -1;
+}
+template <int W>
+__device__ __forceinline__ long long lookup_c(const u64* q, u64 n_pre, const u64* keys, const double* coeffs,
+                                              const u64* table, u64 mask, SweepState* st, double& cj, u64& empty) {
+  const u64 h = key_hash<W>(q);
+  const u32 fp = (u32)(h >> 32);
+  const u64 b = bucket_start(h, mask);
+  const ulonglong2* bp = reinterpret_cast<const ulonglong2*>(table + b);
+  const ulonglong2 s01 = __ldcg(bp), s23 = __ldcg(bp + 1);
+  const u64 sl[4] = {s01.x, s01.y, s23.x, s23.y};
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    if (sl[m] == EMPTY_SLOT) {
+      empty = b + m;
+      return -1;
+    }
+    const u32 row = (u32)sl[m];
+    if ((u32)(sl[m] >> 32) == fp && row < n_pre) {
+      const u64* kp = keys + (u64)row * W;
+      const double c = __ldcg(coeffs + row);
+      bool eq = true;
+#pragma unroll
+      for (int w = 0; w < W; ++w) eq &= __ldcg(kp + w) == q[w];
+      if (eq) {
+        cj = c;
+        return row;
+      }
+    }
+  }
+  return lookup_from_c<W>(q, fp, (b + 4) & mask, n_pre, keys, coeffs, table, mask, st, cj, empty);
+}
+
+// Slot value v for q placed from `start`, the empty slot a lookup of q in
+// this op ended on: the first attempt is the atomic itself, with no load
+// before it; if another key took the slot meanwhile, the probe goes on as in
+// insert.  Returns the slot, or NO_SLOT if the table is full.
+template <int W>
+__device__ u64 place_from(const u64* q, u64 v, u64 start, u64* table, u64 mask, u32* error) {
+  u64 i;
+  if (start != NO_SLOT) {
+    if (atomicCAS(table + start, EMPTY_SLOT, v) == EMPTY_SLOT) return start;
+    i = (start + 1) & mask;
+  } else {
+    i = bucket_start(key_hash<W>(q), mask);
+  }
+  for (u64 probe = 0; probe <= mask; ++probe) {
+    if (__ldcg(table + i) == EMPTY_SLOT && atomicCAS(table + i, EMPTY_SLOT, v) == EMPTY_SLOT) return i;
+    i = (i + 1) & mask;
+  }
+  atomicOr(error, ERR_PROBE_OVERFLOW);
+  return NO_SLOT;
+}
+
 // -(Im phase) of G*K = i^p * sign: the sin-branch multiplier (coeff.rs:151-168).
 __device__ __forceinline__ double neg_im(int p, double sign) {
   return p == 1 ? -sign : (p == 3 ? sign : 0.0);
@@ -434,26 +519,31 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
       if (r < N && Ops::template anticommutes<W>(g, key[k])) anti |= 1u << k;
     }
     n_anti += __popc(anti);
+    // A row's own coefficient is loaded beside its partner lookup, and the
+    // partner's coefficient inside it (lookup_c).
     long long j[IT];
+    double c[IT], cj[IT];
+    u64 es[IT];
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
       j[k] = -1;
+      cj[k] = 0.0;
+      es[k] = NO_SLOT;
       if (!((anti >> k) & 1u)) continue;
+      const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
+      c[k] = __ldcg(coeffs + r);
       u64 q[W];
 #pragma unroll
       for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ g.gen[w];
-      j[k] = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+      j[k] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cj[k], es[k]);
     }
     // The lower row of a pair owns both coefficients.
     u32 own = 0;
-    double c[IT], cj[IT];
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
       const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
       if (!((anti >> k) & 1u) || (j[k] >= 0 && (u64)j[k] < r)) continue;
       own |= 1u << k;
-      c[k] = __ldcg(coeffs + r);
-      cj[k] = j[k] >= 0 ? __ldcg(coeffs + j[k]) : 0.0;
     }
     u32 emit = 0;
     double bval[IT];
@@ -473,7 +563,8 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
         if (si == S_EMIT) {
           emit |= 1u << k;
           bval[k] = bi;
-          slot[k] = claim_slot<W>(q, a.table, a.table_mask, &st->error);
+          slot[k] = place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | PENDING_ROW, es[k], a.table, a.table_mask,
+                                  &st->error);
         }
         if (sm.rec_on) record_single(a, sm, r, c[k]);
       } else {
@@ -547,6 +638,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
     if (t >= ntiles) break;
     u32 emit = 0;
     double bval[IT];
+    u64 eslot[IT];
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
       bval[k] = 0.0;
@@ -556,12 +648,14 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
       load_key<W>(keys, r, key);
       if (!Ops::template anticommutes<W>(g, key)) continue;
       ++n_anti;
+      const double c = __ldcg(coeffs + r);  // beside the lookup, not after it
       u64 q[W];
 #pragma unroll
       for (int w = 0; w < W; ++w) q[w] = key[w] ^ g.gen[w];
-      const long long j = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+      double cj = 0.0;
+      u64 es = NO_SLOT;
+      const long long j = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cj, es);
       if (j >= 0 && (u64)j < r) continue;  // the lower row of the pair owns it
-      const double c = __ldcg(coeffs + r);
       const double bi = __dmul_rn(__dmul_rn(c, sn), neg_im(Ops::template product_exp<W>(g, key), g.sign));
       const int si = a.host_state ? (int)a.host_state[r] : state(c, q);
       if (j < 0) {
@@ -569,10 +663,10 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
         if (si == S_EMIT) {
           emit |= 1u << k;
           bval[k] = bi;
+          eslot[k] = es;
         }
         if (sm.rec_on) record_single(a, sm, r, c);
       } else {
-        const double cj = __ldcg(coeffs + j);
         const double bj = __dmul_rn(__dmul_rn(cj, sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
         const int sj = a.host_state ? (int)a.host_state[j] : state(cj, key);
         const bool to_j = si == S_EMIT || (si == S_HELD && sj == S_EMIT);
@@ -604,7 +698,8 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
       for (int w = 0; w < W; ++w) q[w] ^= g.gen[w];
       store_key<W>(keys, row, q);
       coeffs[row] = bval[k];
-      insert<W>(q, row, a.table, a.table_mask, &st->error);
+      place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | (row & 0xffffffffULL), eslot[k], a.table, a.table_mask,
+                    &st->error);
       if (sm.rec_on) a.rec_idx[sm.rec_base + r] = (u32)row;
     }
     __syncthreads();
@@ -674,20 +769,26 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
 #pragma unroll
       for (int w = 0; w < W; ++w) out[w] = k0[w] ^ ((m & 1) ? d1.g.gen[w] : 0ull) ^ ((m & 2) ? d2.g.gen[w] : 0ull);
     };
+    // The row's own coefficient is loaded beside the member lookups, the
+    // members' coefficients inside them (lookup_c), and each lookup's miss
+    // slot is where that member would be placed.
     long long j[4] = {(long long)r, -1, -1, -1};
+    double cm[4] = {0.0, 0.0, 0.0, 0.0};
+    u64 es[4] = {NO_SLOT, NO_SLOT, NO_SLOT, NO_SLOT};
+    if (a1 || a2) cm[0] = __ldcg(coeffs + r);
     {
       u64 q[W];
       if (a1) {
         member(1, q);
-        j[1] = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+        j[1] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cm[1], es[1]);
       }
       if (a2) {
         member(2, q);
-        j[2] = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+        j[2] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cm[2], es[2]);
       }
       if (a1 && a2) {
         member(3, q);
-        j[3] = lookup<W>(q, N, keys, a.table, a.table_mask, st);
+        j[3] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cm[3], es[3]);
       }
     }
     const bool own = (a1 || a2) && (j[1] < 0 || (u64)j[1] > r) && (j[2] < 0 || (u64)j[2] > r) &&
@@ -702,7 +803,7 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
         p[m] = j[m] >= 0;
-        c[m] = p[m] ? __ldcg(coeffs + j[m]) : 0.0;
+        c[m] = p[m] ? cm[m] : 0.0;
       }
       // One reference step on the pair (x, y) of the family
       // (termsum.rs:604-751): the pair rule if both are present, else the
@@ -761,7 +862,9 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
         bval[m - 1] = c[m];
         u64 q[W];
         member(m, q);
-        slot[m - 1] = claim_slot<W>(q, a.table, a.table_mask, &st->error);  // before the scan: see claim_slot
+        // before the scan: see claim_slot
+        slot[m - 1] = place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | PENDING_ROW, es[m], a.table, a.table_mask,
+                                    &st->error);
         if (born[m] == 1) {
           ++n_born1;
           if (a2) ++n_anti2;  // a row the first rotation creates here anticommutes with the second
