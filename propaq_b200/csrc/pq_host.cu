@@ -854,7 +854,7 @@ int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
   P.rec_key_next = h.rec_key_next;
   P.rec_full = h.rec_full;
   ++P.sweep_launches;
-  if (h.halt != pq::NOT_HALTED) {
+  if (h.halt != pq::NOT_HALTED && !h.grid_stop) {
     u64 ncap = next_pow2(std::max<u64>(4 * P.n_live, 2 * S.cap));
     if (ncap > MAX_ROWS) ncap = MAX_ROWS;
     if (2 * P.n_live > ncap)
@@ -867,18 +867,50 @@ int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
   return PQ_OK;
 }
 
-// Runs every built op of one plan on the whole grid, relaunching after
-// capacity growth.
+// Grid of one sweep launch.  With blocks_per_sm 0 (the default) it follows
+// the live count at the launch: one block per SM while every row has a thread
+// of its own, two per SM up to 2^20 rows, else `max_grid`.  A grid below the
+// largest carries the row count it is chosen for (SweepArgs::grid_rows); the
+// sweep stops before an op that outgrows it and the next launch takes the
+// next size.  Fewer blocks make the grid barrier between ops cheaper (one
+// block per SM took TFIM from 1.95 to 1.74 ms), more blocks keep more rows in
+// flight (the 24-site Majorana run needs them: 35 ms at the largest grid,
+// 76 ms at one block per SM).
+struct GridChoice {
+  int grid;
+  u64 rows;  // 0: no limit
+};
+GridChoice choose_grid(const Plan& P, const Inputs& in, int max_grid) {
+  if (in.cfg->blocks_per_sm != 0) return {max_grid, 0};
+  const auto tier = [&](int bps) {
+    return with_words(P.W, [&](auto w) {
+      constexpr int WW = decltype(w)::value;
+      return P.alg == 0 ? pq::sweep_grid<WW, 0>(bps) : pq::sweep_grid<WW, 1>(bps);
+    });
+  };
+  const int g1 = tier(1), g2 = tier(2);
+  const u64 r1 = (u64)g1 * 256, r2 = 1ULL << 20;
+  if (g1 < max_grid && P.n_live <= r1) return {g1, r1};
+  if (g2 < max_grid && P.n_live <= r2) return {g2, r2};
+  return {max_grid, 0};
+}
+
+// Runs every built op of one plan, relaunching after capacity growth and when
+// the live count outgrows the launch's grid (choose_grid).
 int execute_launches(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size_t op_limit,
                      const Recording* rec, const HostOps* host) {
   cudaError_t e;
   upload_ops(E, S, P);
   const size_t end = std::min(op_limit, P.ops.size());
+  const int max_grid = grid;
   while (P.done < end) {
+    const GridChoice gc = choose_grid(P, *P.in, max_grid);
+    grid = gc.grid;
     E->h_states[0] = fresh_state(P);
     cudaMemcpyAsync(E->d_states, E->h_states, sizeof(pq::SweepState), cudaMemcpyHostToDevice, E->stream);
     cudaMemsetAsync(S.tickets + P.done, 0, (end - P.done) * 4, E->stream);
-    const pq::SweepArgs a = sweep_args(S, P, E->d_states, 0, (u32)grid, end, rec, host);
+    pq::SweepArgs a = sweep_args(S, P, E->d_states, 0, (u32)grid, end, rec, host);
+    a.grid_rows = gc.rows;
     if (!*began) {  // device time starts at the first sweep
       cudaEventRecord(E->ev_begin, E->stream);
       *began = true;

@@ -1051,6 +1051,13 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
       if (grp.bid == 0 && threadIdx.x == 0) st->halt = op;
       break;
     }
+    if (a.grid_rows && N > a.grid_rows) {  // the host relaunches on a larger grid
+      if (grp.bid == 0 && threadIdx.x == 0) {
+        st->halt = op;
+        st->grid_stop = 1;
+      }
+      break;
+    }
     if (a.rec_idx) {
       const bool rec_op = gate_like || od.kind == OP_NOISE_COMPACT;
       if (rec_on && rec_op &&

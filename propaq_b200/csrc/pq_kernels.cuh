@@ -48,6 +48,7 @@ struct SweepState {
   u32 cur;        // row buffer holding the live rows when the sweep ended
   u32 end_op;     // first op the sweep did not run
   u32 yield_after;  // batched: 1 + the op after which the instance stops early (0 = none)
+  u32 grid_stop;  // the sweep stopped at `halt` because the live count outgrew the grid (SweepArgs::grid_rows)
   u32 bar_count;  // grid barrier: groups arrived
   u32 bar_gen;    // grid barrier generation
   static constexpr unsigned BAR_GROUPS = 16;
@@ -75,6 +76,7 @@ struct SweepArgs {
   u64* table;              // open-addressing slots: (fingerprint << 32) | row
   u64 table_mask;
   u64 cap;                 // rows each buffer holds
+  u64 grid_rows;           // stop before an op whose live count exceeds this, 0 = never (see grid_stop)
   u64* status;             // tile look-back status words
   u32* tickets;            // per-op tile counters for many-row gates, zero at entry
   u64* hist;               // live count after each op

@@ -20,6 +20,7 @@ from harness import (
     from_workload,
     golden_fixture,
     golden_problem,
+    make_cfg,
     run_gpu,
     run_oracle,
 )
@@ -374,6 +375,31 @@ def test_capacity_stops_inside_fused_rotations(oracle):
     assert g.res.sweep_launches > 3
     assert np.array_equal(g.n_terms, o.n_terms)
     assert_terms_equal(g.keys, g.coeffs, o.keys, o.coeffs)
+
+
+@pytest.mark.parametrize("make", [lambda: workloads.kicked_ising(6, 6, 6),
+                                  lambda: workloads.majorana_givens(n_sites=12, reps=2, seed=4)],
+                         ids=["kicked6x6", "majorana12"])
+def test_grid_follows_the_live_count(gpu_engine, oracle, make):
+    # The default grid starts at one block per SM and the sweep stops and is
+    # relaunched on a larger grid as the live count grows past 148 x 256 rows
+    # (and past 2^20); a fixed grid runs without those stops.  Both give the
+    # oracle's terms and counts.
+    p = from_workload(make())
+    run_gpu(gpu_engine, p)  # the engine's buffers grow to size here
+    cfg, keep = make_cfg(p)
+    auto = run_gpu(gpu_engine, p)
+    cfg.blocks_per_sm = 3
+    res, nt = gpu_engine.run(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag)
+    keys, coeffs = gpu_engine.terms(p.n_words)
+    assert auto.res.peak_terms > 148 * 256
+    assert auto.res.sweep_launches > res.sweep_launches, "the default grid must have grown during the run"
+    o = run_oracle(oracle, p)
+    for n_terms, k, c in ((auto.n_terms, auto.keys, auto.coeffs), (nt, keys, coeffs)):
+        assert np.array_equal(n_terms, o.n_terms)
+        assert_terms_equal(k, c, o.keys, o.coeffs)
+    ok, _, _ = expectation_close(auto.expectation, o)
+    assert ok
 
 
 def test_width_errors(gpu_engine):
