@@ -61,7 +61,7 @@ def parse():
                              "batch_small", "adjoint", "adjoint_small"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--blocks-per-sm", type=int, default=0, help="sweep blocks per SM (0 = as many as fit)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="sweep blocks per SM (0 = by live count; batch: as many as fit)")
     ap.add_argument("--split", type=int, default=1, help="batch: 0 equal grid shares, 1 by remaining work")
     ap.add_argument("--rebalance-pct", type=int, default=25, help="batch: re-split when this %% of the grid idles")
     ap.add_argument("--no-sequential", action="store_true", help="batch: skip the sequential pq_run comparison")

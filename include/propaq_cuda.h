@@ -81,7 +81,10 @@ typedef struct pq_run_config {
   size_t noise_table_len;    /* entries per table (normally n_units + 1)       */
   const pq_plugin* noise_plugin; /* PLUGIN kind                                 */
   uint32_t want_terms;       /* keep the final terms for pq_result_terms        */
-  uint32_t blocks_per_sm;    /* sweep blocks per SM; 0 = as many as fit (tuning) */
+  uint32_t blocks_per_sm;    /* sweep blocks per SM; 0 = by live count: 1 while
+                                every row has a thread, 2 up to 2^20 rows, then
+                                as many as fit (a launch stops and is relaunched
+                                when its live count outgrows its grid)          */
 } pq_run_config;
 
 /* crates/core/src/interface/results.rs:8-51 (PropagationResult), plus the
