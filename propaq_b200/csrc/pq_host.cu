@@ -645,6 +645,8 @@ int build_ops(Plan& P, NeedN need_n) {
   const Inputs& in = *P.in;
   const int W = P.W, ALG = P.alg;
   std::vector<u64> g(W), gc(W);
+  P.gdesc.reserve(P.gdesc.size() + in.n_gates * gdesc_words(W));
+  P.ops.reserve(P.ops.size() + in.n_gates + in.n_layers);
   for (size_t l = 0; l < in.n_layers; ++l) {
     P.layer_op.push_back(P.ops.size());
     if (P.have_noise) {
@@ -1274,7 +1276,6 @@ int run_one(pq_engine* E, const Inputs& in, int W) {
   return PQ_OK;
 }
 
-// Device buffers of one adjoint run, freed on every exit path.
 // Expectation value and dE/d(angle) of every gate with the truncation
 // decisions of the forward run held fixed.  The forward run records each op
 // (SweepArgs::rec_idx: sin-branch partners, pre-op coefficients, reclaim maps

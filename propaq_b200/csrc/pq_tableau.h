@@ -101,6 +101,26 @@ inline int rotated_sign(double sn, int p) {
   return sn * nim < 0 ? -1 : 1;
 }
 
+// Calls f(p) for every unit bit p < lim that can anticommute with gen: for a
+// Pauli generator only the X and Z bits of the qubits it acts on (a unit on
+// any other qubit commutes with it), for a Majorana generator every bit.
+template <class F>
+inline void for_candidate_units(int alg, int W, const u64* gen, size_t lim, F f) {
+  if (alg != 0) {
+    for (size_t p = 0; p < lim; ++p) f(p);
+    return;
+  }
+  for (int wi = 0; wi < W; ++wi) {
+    u64 sup = (gen[wi] | (gen[wi] >> 1)) & EVEN;
+    while (sup) {
+      const size_t p = (size_t)wi * 64 + __builtin_ctzll(sup);
+      sup &= sup - 1;
+      if (p < lim) f(p);
+      if (p + 1 < lim) f(p + 1);
+    }
+  }
+}
+
 // --------------------------------------------------------------- tableau
 // A deferred Clifford frame (crates/core/src/algebra/tableau.rs:29-223):
 // 2n rows, a readout map P -> C^dag P C and its inverse generator map.
@@ -218,18 +238,18 @@ struct Tableau {
     std::vector<u64> imgs;
     std::vector<int> sgns;
     u64 e[MAX_WORDS] = {0}, m[MAX_WORDS];
-    for (size_t p = 0; p < lim; ++p) {
+    for_candidate_units(alg, W, gen, lim, [&](size_t p) {
       e[p / 64] = 1ULL << (p % 64);
       const bool anti = host_anticommutes(alg, W, gen, e);
       const int pe = anti ? host_product_exp(alg, W, gen, e) : 0;
       e[p / 64] = 0;
-      if (!anti) continue;
+      if (!anti) return;
       for (int i = 0; i < W; ++i) m[i] = gen[i];
       m[p / 64] ^= 1ULL << (p % 64);
       changed.push_back(p);
       imgs.resize(imgs.size() + W);
       sgns.push_back(apply(gen_img, gen_sign, m, &imgs[imgs.size() - W]) * -rotated_sign(sn, pe));
-    }
+    });
     for (size_t c = 0; c < changed.size(); ++c) {
       std::memcpy(&gen_img[changed[c] * W], &imgs[c * W], 8 * W);
       gen_sign[changed[c]] = sgns[c];
@@ -242,16 +262,18 @@ struct Tableau {
   static bool rotation_changes_weight(int alg, int W, u32 n_units, const u64* gen) {
     const size_t lim = std::min((size_t)2 * n_units, (size_t)64 * W);
     u64 e[MAX_WORDS] = {0}, img[MAX_WORDS];
-    for (size_t p = 0; p < lim; ++p) {
+    bool changes = false;
+    for_candidate_units(alg, W, gen, lim, [&](size_t p) {
+      if (changes) return;
       e[p / 64] = 1ULL << (p % 64);
       const bool anti = host_anticommutes(alg, W, gen, e);
       e[p / 64] = 0;
-      if (!anti) continue;
+      if (!anti) return;
       for (int i = 0; i < W; ++i) img[i] = gen[i];
       img[p / 64] ^= 1ULL << (p % 64);
-      if (host_support(W, img) != 1) return true;
-    }
-    return false;
+      if (host_support(W, img) != 1) changes = true;
+    });
+    return changes;
   }
 };
 

@@ -1,7 +1,8 @@
 // Checks the deferred Clifford frame's direct rotation update
 // (Tableau::compose_rotation) against full composition with the rotation's
-// tableau (Tableau::compose(Tableau::for_rotation(...))) on random Clifford
-// sequences, Pauli and Majorana, 1 and 2 key words: both maps, every row,
+// tableau (Tableau::compose(Tableau::for_rotation(...))), and
+// Tableau::rotation_changes_weight against the rotation's full tableau, on
+// random Clifford sequences, Pauli and Majorana, 1 and 2 key words: both maps, every row,
 // every sign, and the conjugated generators of random rotations after each
 // step.  Built and run by test_tableau_cpu.py; prints "ok" or the first
 // difference.
@@ -40,8 +41,19 @@ int main() {
             u64 g[MAX_WORDS];
             random_key(rng, alg, W, n_units, step % 5 == 4 ? (int)n_units : 3, g);
             const double ang = (rng() & 1) ? M_PI / 2 : -M_PI / 2;
+            const Tableau rt = Tableau::for_rotation(alg, W, n_units, g, ang);
+            bool want = false;  // a unit row whose image has another support
+            for (size_t p = 0; p < rt.rows; ++p) {
+              u64 u[MAX_WORDS] = {0};
+              if (p < (size_t)64 * W) u[p / 64] = 1ULL << (p % 64);
+              if (host_support(W, &rt.rd_img[p * W]) != host_support(W, u)) want = true;
+            }
+            if (Tableau::rotation_changes_weight(alg, W, n_units, g) != want) {
+              std::printf("weight change differs: alg %d W %d n %u seq %d step %d\n", alg, W, n_units, seq, step);
+              return 1;
+            }
             fast.compose_rotation(g, ang);
-            full.compose(Tableau::for_rotation(alg, W, n_units, g, ang));
+            full.compose(rt);
             ++cases;
             if (!same(fast, full)) {
               std::printf("frame differs: alg %d W %d n %u seq %d step %d\n", alg, W, n_units, seq, step);
