@@ -46,18 +46,19 @@ def heisenberg_gates(circuit, n_words: int, key_of):
     """Flattens circuit.layers into arrays in Heisenberg order: layers reversed and
     the gates within each layer reversed (crates/pauli/src/engine.rs:44-70).
     Returns (gate_words [G, n_words], angles [G], layer_offsets [L+1])."""
-    layers = list(circuit.layers)
-    gens, angles, offsets = [], [], [0]
-    for layer in reversed(layers):
-        for rot in reversed(list(layer)):
-            gens.append(key_of(rot.generator))
-            angles.append(float(rot.angle))
-        offsets.append(len(angles))
-    return keys_to_words(gens, n_words), np.array(angles, dtype=np.float64), np.array(offsets, dtype=np.uint32)
+    rots, offsets = [], [0]
+    for layer in reversed(list(circuit.layers)):
+        rots.extend(layer[::-1] if isinstance(layer, (list, tuple)) else list(layer)[::-1])
+        offsets.append(len(rots))
+    keys = [key_of(r.generator) for r in rots]
+    angles = np.fromiter((r.angle for r in rots), dtype=np.float64, count=len(rots))
+    return keys_to_words(keys, n_words), angles, np.array(offsets, dtype=np.uint32)
 
 
 def keys_to_words(keys, n_words: int) -> np.ndarray:
     """Python-int keys -> [len, n_words] little-endian u64 words."""
+    if n_words == 1:
+        return np.fromiter(keys, dtype=np.uint64, count=len(keys)).reshape(len(keys), 1)
     nb = 8 * n_words
     buf = b"".join(k.to_bytes(nb, "little") for k in keys)
     return np.frombuffer(buf, dtype="<u8").reshape(len(keys), n_words).astype(np.uint64)
@@ -198,7 +199,7 @@ class _Propagator:
             from .term_io import save_terms
 
             save_terms(filename, terms[0], terms[1], self._basis, self._n_units_io(observable))
-        return PropagationResult(res.expectation_value, [int(x) for x in nt], res.sparse_key_bytes,
+        return PropagationResult(res.expectation_value, nt.tolist(), res.sparse_key_bytes,
                                  res.terms_below_cutoff)
 
     def _n_units_io(self, observable) -> int:
