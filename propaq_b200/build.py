@@ -13,13 +13,17 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libpropaq_cuda.so"
-SOURCES = ["pq_kernels.cu", "pq_host.cu", "pq_noalloc.cu"]
+# The 16-, 32- and 64-word kernels are separate translation units (they
+# include pq_kernels.cu) so that they compile in parallel with the rest.
+SOURCES = ["pq_kernels_w64.cu", "pq_kernels_w32.cu", "pq_kernels_w16.cu", "pq_kernels.cu", "pq_host.cu",
+           "pq_noalloc.cu"]
 HEADERS = ["pq_device.cuh", "pq_kernels.cuh", "pq_tableau.h"]
 
 NVCC_FLAGS = [
@@ -51,17 +55,22 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not _stale():
         return LIB
     LIB_DIR.mkdir(exist_ok=True)
-    objs = []
-    for src in SOURCES:
+
+    def compile_one(src):
         obj = LIB_DIR / (Path(src).stem + ".o")
         cmd = [nvcc(), *NVCC_FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, str(obj), subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as pool:
+        results = list(pool.map(compile_one, SOURCES))
+    objs = []
+    for src, obj, r in results:
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError(f"nvcc failed on {src}")
         if verbose:
             sys.stderr.write(r.stderr)
-        objs.append(str(obj))
+        objs.append(obj)
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", str(tmp), "-ldl"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -53,7 +53,7 @@ struct GenInfo {
   u64 gen[W];    // generator key (after the Clifford frame)
   u64 fold[W];   // Pauli: pair-swapped generator; Majorana: the generator
   u64 sfx[W];    // Majorana: per word, parity of generator bits strictly above each bit
-  u32 carry;     // Majorana: bit w = parity of generator bits in words above w
+  u64 carry;     // Majorana: bit w = parity of generator bits in words above w (W <= 64)
   int aux;       // Pauli: Y sites of the generator; Majorana: its length
   double sign;   // +1 / -1 carried by the generator from the frame
 };
@@ -129,7 +129,7 @@ struct MajoranaOps {
       int pk = popc(k[i]);
       lk += pk;
       lo += popc(o);
-      sw ^= (popc(k[i] & g.sfx[i]) & 1) ^ (pk & (int)((g.carry >> i) & 1u));
+      sw ^= (popc(k[i] & g.sfx[i]) & 1) ^ (pk & (int)((g.carry >> i) & 1ull));
     }
     return mod4(herm(g.aux) + herm(lk) - herm(lo) + 2 * (sw & 1));
   }

@@ -147,7 +147,10 @@ decltype(auto) with_words(int W, F&& f) {
     case 1: return f(std::integral_constant<int, 1>{});
     case 2: return f(std::integral_constant<int, 2>{});
     case 4: return f(std::integral_constant<int, 4>{});
-    default: return f(std::integral_constant<int, 8>{});
+    case 8: return f(std::integral_constant<int, 8>{});
+    case 16: return f(std::integral_constant<int, 16>{});
+    case 32: return f(std::integral_constant<int, 32>{});
+    default: return f(std::integral_constant<int, 64>{});
   }
 }
 
@@ -425,7 +428,7 @@ pq::GenInfo<W> make_gen(int alg, const u64* g, int sign) {
     u64 s = g[i] >> 1;
     for (int sh = 1; sh < 64; sh <<= 1) s ^= s >> sh;
     gi.sfx[i] = s;
-    if (above) gi.carry |= 1u << i;
+    if (above) gi.carry |= 1ull << i;
     above ^= hpopc(g[i]) & 1;
   }
   return gi;
@@ -1701,9 +1704,6 @@ int check_inputs(pq_engine* E, const pq_run_config* cfg, size_t ng, const uint32
   if (!W)
     return E->fail(PQ_ERR_INVALID, "propaq: " + std::to_string(cfg->n_units) +
                                        " units exceeds the engine's maximum of 2048");
-  if (W > 8)
-    return E->fail(PQ_ERR_UNSUPPORTED, "registers wider than 256 units (" + std::to_string(W) +
-                                           " words) are not compiled into this build");
   if (nl && (!lo || lo[0] != 0 || lo[nl] != ng)) return E->fail(PQ_ERR_INVALID, "layer offsets do not cover the gates");
   if (!nl && ng) return E->fail(PQ_ERR_INVALID, "layer offsets do not cover the gates");
   for (size_t l = 0; l < nl; ++l)

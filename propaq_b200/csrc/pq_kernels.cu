@@ -1559,6 +1559,7 @@ cudaError_t launch_adjoint_seed(const ExpectArgs& a, const u64* keys, u64 n, dou
   return cudaGetLastError();
 }
 
+#ifndef PQ_ONLY_WIDTH  // defined once, in the translation unit of the narrow widths
 cudaError_t launch_grad_reduce(const double* grad_part, int grid, const long long* gate_ops, u64 n_gates,
                                double* grad, cudaStream_t s) {
   if (!n_gates) return cudaSuccess;
@@ -1567,6 +1568,7 @@ cudaError_t launch_grad_reduce(const double* grad_part, int grid, const long lon
                                                                                   grad);
   return cudaGetLastError();
 }
+#endif
 
 template <int W, int ALG>
 int adjoint_grid() {
@@ -1619,9 +1621,17 @@ cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const
   template cudaError_t launch_conjugate<Wv>(const u64*, const double*, u64, const u64*, const int*, u32, int, \
                                             u64*, double*, cudaStream_t);
 
+// Key widths 1-8 words (up to 256 units) here; 16, 32 and 64 words each in a
+// translation unit of its own (pq_kernels_w16.cu ...) that defines
+// PQ_ONLY_WIDTH and includes this file, so that the widths compile in
+// parallel.
+#ifdef PQ_ONLY_WIDTH
+PQ_INSTANTIATE_W(PQ_ONLY_WIDTH)
+#else
 PQ_INSTANTIATE_W(1)
 PQ_INSTANTIATE_W(2)
 PQ_INSTANTIATE_W(4)
 PQ_INSTANTIATE_W(8)
+#endif
 
 }  // namespace pq

@@ -1,0 +1,4 @@
+// The engine's kernels for 64-word keys (1025-2048 units), compiled in a
+// translation unit of their own so that the key widths build in parallel.
+#define PQ_ONLY_WIDTH 64
+#include "pq_kernels.cu"

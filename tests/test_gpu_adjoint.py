@@ -97,6 +97,19 @@ def test_gradient_matches_forward_mode_reference(gpu_engine, oracle, case, seed)
     np.testing.assert_allclose(g2, g_ref, rtol=1e-9, atol=1e-12 * scale)
 
 
+def test_gradient_on_a_wide_register(gpu_engine, oracle):
+    # 64-word keys (2048 qubits), 10 active qubits spread over the register.
+    from test_gpu_parity import random_pauli_problem, spread_units
+
+    p = random_pauli_problem(4, 2048, n_gates=50, clifford_frac=0.0, units=spread_units(4, 2048, 10), max_weight=4,
+                             min_coeff=1e-3)
+    e_ref, g_ref = propagate_with_tangents(oracle, p)
+    res, nt, g = gpu_grad(gpu_engine, p, checkpoint_layers=2)
+    assert abs(res.expectation_value - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
+    scale = max(1.0, float(np.abs(g_ref).max()))
+    np.testing.assert_allclose(g, g_ref, rtol=1e-9, atol=1e-12 * scale)
+
+
 @pytest.mark.parametrize("wl", [workloads.hardware_efficient(12, 5, seed=2), workloads.kicked_ising(4, 5, 4)],
                          ids=["hea", "kicked_noisy"])
 def test_recording_in_the_forward_pass_equals_replayed_segments(gpu_engine, wl):

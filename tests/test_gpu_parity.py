@@ -218,12 +218,14 @@ def test_python_term_hook_errors_propagate(gpu_engine):
 
 
 # ------------------------------------------------------------ random circuits
-def random_pauli_problem(seed, n, n_gates=60, layer_size=4, clifford_frac=0.15, **kw):
+def random_pauli_problem(seed, n, n_gates=60, layer_size=4, clifford_frac=0.15, units=None, **kw):
+    """Random rotations on 1-3 qubits; with `units`, gates and observable act
+    on those qubits only (a few qubits spread over a wide register)."""
     rng = np.random.default_rng(seed)
     layers, layer = [], []
     for _ in range(n_gates):
         k = int(rng.integers(1, 4))
-        qs = rng.choice(n, size=k, replace=False)
+        qs = rng.choice(n, size=k, replace=False) if units is None else rng.choice(units, size=k, replace=False)
         x = z = 0
         for q in qs:
             t = int(rng.integers(1, 4))
@@ -243,11 +245,15 @@ def random_pauli_problem(seed, n, n_gates=60, layer_size=4, clifford_frac=0.15, 
     if layer:
         layers.append(layer)
     obs = PauliTermSum()
+    pick = (lambda: int(rng.integers(0, n))) if units is None else (lambda: int(rng.choice(units)))
     for _ in range(3):
-        q = int(rng.integers(0, n))
+        q = pick()
         obs.add(PauliString(0, 1 << q, n), float(rng.normal()))
-    obs.add(PauliString(0, (1 << int(rng.integers(0, n))) | 1, n), 0.5)
-    return from_circuit(0, n, obs, PauliCircuit(layers), int(rng.integers(0, 1 << min(n, 62))), **kw)
+    obs.add(PauliString(0, (1 << pick()) | (1 if units is None else 1 << int(units[0])), n), 0.5)
+    state = int(rng.integers(0, 1 << min(n, 62)))
+    if units is not None:
+        state |= sum(int(rng.integers(0, 2)) << int(q) for q in units)
+    return from_circuit(0, n, obs, PauliCircuit(layers), state, **kw)
 
 
 PAULI_CASES = [
@@ -283,26 +289,49 @@ def test_random_pauli_with_noise(gpu_engine, oracle, seed):
     check(gpu_engine, oracle, q)
 
 
-def random_majorana_problem(seed, n_sites, n_gates=50, **kw):
+def spread_units(seed, n, k):
+    """k units spread over a register of n: one in each of k equal stretches."""
+    rng = np.random.default_rng(1000 + seed)
+    edges = np.linspace(0, n, k + 1).astype(int)
+    return [int(rng.integers(edges[i], edges[i + 1])) for i in range(k)]
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+@pytest.mark.parametrize("n", [300, 700, 2048], ids=["W16", "W32", "W64"])
+def test_wide_registers(gpu_engine, oracle, n, seed):
+    # 16-, 32- and 64-word keys (257-2048 qubits): 12 active qubits spread
+    # over the whole register, so keys and generators span every word.
+    p = random_pauli_problem(seed, n, n_gates=80, units=spread_units(seed, n, 12), max_weight=6, min_coeff=1e-4)
+    g, o = check(gpu_engine, oracle, p)
+    assert max(g.n_terms) > 100
+
+
+def random_majorana_problem(seed, n_sites, n_gates=50, sites=None, **kw):
+    """Random Givens, number-number and single-mode rotations; with `sites`,
+    gates and observable act on those sites only."""
     rng = np.random.default_rng(seed)
     n_modes = 2 * n_sites
     rots = []
     for _ in range(n_gates):
         kind = rng.random()
-        i, j = sorted(int(v) for v in rng.choice(n_sites, size=2, replace=False))
+        pool = n_sites if sites is None else sites
+        i, j = sorted(int(v) for v in rng.choice(pool, size=2, replace=False))
         if kind < 0.4:
             rots += pq.circuits.majorana_xx_plus_yy(i, j, float(rng.uniform(-math.pi, math.pi)), n_modes)
         elif kind < 0.8:
             rots += pq.circuits.majorana_cp(i, j, float(rng.normal(0, 0.5)), n_modes)
         else:  # an odd-length generator (exercises the odd anticommutation fold)
-            m = 1 << int(rng.integers(0, n_modes))
+            m = 1 << (int(rng.integers(0, n_modes)) if sites is None else 2 * int(rng.choice(sites)) + int(rng.integers(0, 2)))
             rots.append(MajoranaRotation(MajoranaMonomial(m, n_modes, False), float(rng.uniform(-1, 1))))
     layers = [rots[k:k + 5] for k in range(0, len(rots), 5)]
     obs = MajoranaTermSum()
     for _ in range(4):
-        s = int(rng.integers(0, n_sites))
+        s = int(rng.integers(0, n_sites)) if sites is None else int(rng.choice(sites))
         obs.add(MajoranaMonomial(3 << (2 * s), n_modes), float(rng.normal()))
-    return from_circuit(1, n_sites, obs, MajoranaCircuit(layers), int(rng.integers(0, 1 << min(n_sites, 62))), **kw)
+    state = int(rng.integers(0, 1 << min(n_sites, 62)))
+    if sites is not None:
+        state |= sum(int(rng.integers(0, 2)) << int(q) for q in sites)
+    return from_circuit(1, n_sites, obs, MajoranaCircuit(layers), state, **kw)
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])
@@ -313,6 +342,25 @@ def test_random_majorana(gpu_engine, oracle, case, seed):
     case = dict(case)
     n = case.pop("n")
     check(gpu_engine, oracle, random_majorana_problem(seed, n, **case))
+
+
+@pytest.mark.parametrize("n", [400, 2048], ids=["W16", "W64"])
+def test_wide_majorana(gpu_engine, oracle, n):
+    check(gpu_engine, oracle, random_majorana_problem(3, n, n_gates=60, sites=spread_units(3, n, 9), max_weight=6,
+                                                      min_coeff=1e-4))
+
+
+def test_wide_registers_in_a_batch(gpu_engine, oracle):
+    # A 64-word instance with 8-, 4- and 1-word ones: the narrow keys are
+    # widened to the batch's width (results unchanged).
+    probs = [random_pauli_problem(s, n, n_gates=60, units=spread_units(s, n, 10), max_weight=5, min_coeff=1e-4)
+             for s, n in ((5, 2048), (6, 200), (7, 100), (8, 20))]
+    from harness import run_gpu_batch
+
+    for p, b in zip(probs, run_gpu_batch(gpu_engine, probs)):
+        o = run_oracle(oracle, p)
+        assert np.array_equal(b.n_terms, o.n_terms)
+        assert_terms_equal(b.keys, b.coeffs, o.keys, o.coeffs)
 
 
 # ------------------------------------------------------------ configurations
