@@ -675,10 +675,16 @@ def main():
     # The dominant kernel is the sweep: one cooperative launch per step (plus
     # one per capacity growth) runs every gate and noise op.
     achieved = alg_bytes / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else None
+    # DRAM bytes of the sweep launches of one step, from an ncu capture
+    # (profiles/sweep_traffic_*.json), as bytes per launch like `achieved`:
+    # the step's bytes over the launches a step took here (the grid follows
+    # the live count, so a step can be several launches).
     traffic = None
     tf = ROOT / "profiles" / f"sweep_traffic_{wl.name}.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
+    if tf.exists() and sweep_launches:
+        per_step = json.loads(tf.read_text()).get("dram_bytes_per_step")
+        if per_step is not None:
+            traffic = per_step / (sweep_launches / args.steps)
     line = dict(base_line, value=value, ms_per_step=1e3 * dev_s / args.steps,
                 e2e={"value": e2e_value, "unit": "terms/s", "h2d_bytes_per_step": int(h2d),
                      "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s / args.steps},
