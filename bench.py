@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--split", type=int, default=1, help="batch: 0 equal grid shares, 1 by remaining work")
     ap.add_argument("--rebalance-pct", type=int, default=25, help="batch: re-split when this %% of the grid idles")
     ap.add_argument("--no-sequential", action="store_true", help="batch: skip the sequential pq_run comparison")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batch: time the given --blocks-per-sm/--split/--rebalance-pct instead of the autotuner's")
     ap.add_argument("--checkpoint-layers", type=int, default=3, help="adjoint: layers per checkpoint segment")
     ap.add_argument("--shift-sample", type=int, default=96, help="adjoint: parameter-shift evaluations timed")
     return ap.parse_args()
@@ -311,6 +313,16 @@ def main_batch(args, world, rank, local):
     for _ in range(args.warmup):
         settle()
         engine.run_batch(items, **tune)
+    tuned = None
+    if not args.no_autotune:
+        # The project's autotuner picks the launch parameters by measurement
+        # (propaq_b200.tuning), once per batch shape, before the timed region.
+        from propaq_b200.tuning import batch_signature, default_tuner
+
+        tuner = default_tuner()
+        t = tuner.tune(items, local)
+        tune = t.as_dict()
+        tuned = [dict(c.as_dict(), device_ms=ms) for c, ms in tuner.trials[batch_signature(items)]]
     for _ in range(min(1, args.warmup)):
         settle()
         expectation_values(jobs, **tune)
@@ -368,7 +380,7 @@ def main_batch(args, world, rank, local):
                           "kernel": "batch_sweep_kernel", "peak_source": f"{peak_kind} hbm_gbs",
                           "launches_per_step": sweep_launches / max(1, args.steps),
                           "share_of_device_time": sweep_ms / dev_ms if dev_ms else None},
-                tuning=tune, clocks=clocks)
+                tuning=dict(tune, autotuned=tuned is not None, trials=tuned), clocks=clocks)
     if seq_ms:
         line["sequential"] = {"what": "the same 64 instances as pq_run calls one after another, same GPU",
                               "value": seq_terms / (seq_ms / 1e3), "ms_per_step": seq_ms / args.steps,

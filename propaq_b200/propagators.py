@@ -206,7 +206,8 @@ class _Propagator:
         return observable.n_units()
 
 
-def expectation_values(jobs, blocks_per_sm: int = 0, split: int = 1, rebalance_pct: int = 25, device: int = 0):
+def expectation_values(jobs, blocks_per_sm: int = 0, split: int = 1, rebalance_pct: int = 25, device: int = 0,
+                       autotune: bool = False):
     """Expectation values of many independent propagations in shared
     persistent launches on one GPU (pq_run_batch).
 
@@ -220,7 +221,9 @@ def expectation_values(jobs, blocks_per_sm: int = 0, split: int = 1, rebalance_p
     blocks_per_sm: grid size per SM (0 = as many as fit); split: 0 shares the
     grid equally among the jobs, 1 in proportion to their remaining work;
     rebalance_pct: re-split the grid among the running jobs once this share of
-    it is idle (0 = never).
+    it is idle (0 = never).  autotune: choose these three by measurement
+    instead (propaq_b200.tuning; the first batch of a shape runs once per
+    candidate setting, later ones reuse the choice).
     """
     jobs = list(jobs)
     if not jobs:
@@ -231,11 +234,16 @@ def expectation_values(jobs, blocks_per_sm: int = 0, split: int = 1, rebalance_p
         items.append(args)
         keep.append(k)
     eng = _native.engine(device)
+    if autotune:
+        from .tuning import default_tuner
+
+        t = default_tuner().tune(items, device)
+        blocks_per_sm, split, rebalance_pct = t.blocks_per_sm, t.split, t.rebalance_pct
     out = eng.run_batch(items, blocks_per_sm=blocks_per_sm, split=split, rebalance_pct=rebalance_pct)
     results = []
     for (prop, *_), (res, nt) in zip(jobs, out):
         prop.last_run = res
-        results.append(PropagationResult(res.expectation_value, [int(x) for x in nt], res.sparse_key_bytes,
+        results.append(PropagationResult(res.expectation_value, nt.tolist(), res.sparse_key_bytes,
                                          res.terms_below_cutoff))
     return results
 

@@ -137,6 +137,35 @@ def test_expectation_values_api(gpu_engine):
         assert r.terms_below_cutoff == s.terms_below_cutoff
 
 
+def test_autotuned_batch(gpu_engine):
+    # The autotuner runs the batch once per candidate setting and keeps the
+    # fastest; any setting gives every instance its pq_run result, and the
+    # propagator-level call with autotune=True reuses the remembered choice.
+    from harness import make_cfg
+
+    from propaq_b200.tuning import CANDIDATES, BatchTuner, batch_signature
+
+    probs = mixed_problems()[:4]
+    items, keep = [], []
+    for p in probs:
+        cfg, k = make_cfg(p, want_terms=False)
+        keep.append(k)
+        items.append((cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag))
+    tuner = BatchTuner()
+    t = tuner.tune(items)
+    assert (t.blocks_per_sm, t.split, t.rebalance_pct) in CANDIDATES
+    assert len(tuner.trials[batch_signature(items)]) == len(CANDIDATES)
+    for b, p in zip(run_gpu_batch(gpu_engine, probs, **t.as_dict()), probs):
+        assert_same(b, run_gpu(gpu_engine, p))
+    wl = workloads.kicked_ising(5, 6, 4)
+    jobs = [(pq.PauliPropagator(noise=pq.UniformNoiseModel(d), truncation=wl.truncation()), wl.observable, wl.circuit, 0)
+            for d in (1e-3, 2e-3)]
+    for r, (prop, o, c, s) in zip(expectation_values(jobs, autotune=True), jobs):
+        single = prop.expectation_value(o, c, s)
+        assert close(r.expectation_value, single.expectation_value)
+        assert r.n_terms == single.n_terms
+
+
 def test_batch_refusals(gpu_engine):
     wl = workloads.kicked_ising(4, 4, 2)
     maj = workloads.majorana_givens(n_sites=8, reps=1)

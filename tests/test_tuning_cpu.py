@@ -1,0 +1,40 @@
+"""The batch autotuner's choice and memory (propaq_b200.tuning), with a fake
+run in place of the GPU."""
+
+from types import SimpleNamespace
+
+import numpy as np
+
+from propaq_b200.tuning import CANDIDATES, BatchTuner, Tuning, batch_signature
+
+
+def item(n_units, n_gates, max_weight=10, angle=0.3):
+    cfg = SimpleNamespace(basis_kind=0, n_units=n_units, max_weight=max_weight, has_min_coeff=1, min_coeff=1e-5,
+                          min_terms=-1, noise_kind=1)
+    return (cfg, np.zeros((1, 1), np.uint64), np.ones(1), np.zeros((n_gates, 1), np.uint64),
+            np.full(n_gates, angle), np.array([0, n_gates], np.uint32), None)
+
+
+def test_picks_the_fastest_candidate_and_remembers_it_per_shape():
+    times = {c: 10.0 + i for i, c in enumerate(CANDIDATES)}
+    times[(0, 1, 50)] = 3.0
+    calls = []
+
+    def run(items, t):
+        calls.append(t)
+        return times[(t.blocks_per_sm, t.split, t.rebalance_pct)]
+
+    tuner = BatchTuner()
+    batch = [item(40, 100), item(90, 300)]
+    assert tuner.tune(batch, run=run) == Tuning(0, 1, 50)
+    assert len(calls) == len(CANDIDATES)
+    # the same shape with other angles: remembered, no new runs
+    again = [item(40, 100, angle=0.9), item(90, 300, angle=0.1)]
+    assert tuner.tune(again, run=run) == Tuning(0, 1, 50)
+    assert len(calls) == len(CANDIDATES)
+    assert tuner.choice(again) == Tuning(0, 1, 50)
+    # another shape is tuned on its own
+    other = [item(40, 100, max_weight=8)]
+    assert batch_signature(other) != batch_signature(batch)
+    tuner.tune(other, run=run)
+    assert len(calls) == 2 * len(CANDIDATES)
