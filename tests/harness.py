@@ -10,6 +10,7 @@ from pathlib import Path
 import numpy as np
 
 from propaq_b200 import _native
+from propaq_b200.circuits import PauliCircuit, PauliRotation
 from propaq_b200.datatypes import PauliString, PauliTermSum
 from propaq_b200.propagators import heisenberg_gates, state_words
 
@@ -72,8 +73,6 @@ def golden_fixture():
 
 def golden_problem(**kw) -> Problem:
     """The plugin notebooks' 4-qubit, 40-rotation circuit, one rotation per layer."""
-    from propaq_b200.circuits import PauliCircuit, PauliRotation
-
     fx = golden_fixture()
     n = fx["n_qubits"]
     circ = PauliCircuit([PauliRotation(PauliString(r["x"], r["z"], n), r["angle"]) for r in fx["rotations"]])
@@ -175,3 +174,48 @@ def expectation_close(gpu_value, oracle_result, rel=1e-12):
     ref = oracle_result.expectation_accurate
     tol = rel * abs(ref) + 4 * np.finfo(float).eps * oracle_result.expectation_abs
     return abs(gpu_value - ref) <= tol, abs(gpu_value - ref), tol
+
+
+def spread_units(seed, n, k):
+    """k units spread over a register of n: one in each of k equal stretches."""
+    rng = np.random.default_rng(1000 + seed)
+    edges = np.linspace(0, n, k + 1).astype(int)
+    return [int(rng.integers(edges[i], edges[i + 1])) for i in range(k)]
+
+
+def random_pauli_problem(seed, n, n_gates=60, layer_size=4, clifford_frac=0.15, units=None, **kw):
+    """Random rotations on 1-3 qubits; with `units`, gates and observable act
+    on those qubits only (a few qubits spread over a wide register)."""
+    rng = np.random.default_rng(seed)
+    layers, layer = [], []
+    for _ in range(n_gates):
+        k = int(rng.integers(1, 4))
+        qs = rng.choice(n, size=k, replace=False) if units is None else rng.choice(units, size=k, replace=False)
+        x = z = 0
+        for q in qs:
+            t = int(rng.integers(1, 4))
+            x |= (t & 1) << int(q)
+            z |= (t >> 1) << int(q)
+        r = rng.random()
+        if r < clifford_frac:
+            a = float(rng.choice([math.pi / 2, -math.pi / 2, 3 * math.pi / 2]))
+        elif r < clifford_frac + 0.05:
+            a = math.pi
+        else:
+            a = float(rng.uniform(-1.2, 1.2))
+        layer.append(PauliRotation(PauliString(x, z, n), a))
+        if len(layer) == layer_size:
+            layers.append(layer)
+            layer = []
+    if layer:
+        layers.append(layer)
+    obs = PauliTermSum()
+    pick = (lambda: int(rng.integers(0, n))) if units is None else (lambda: int(rng.choice(units)))
+    for _ in range(3):
+        q = pick()
+        obs.add(PauliString(0, 1 << q, n), float(rng.normal()))
+    obs.add(PauliString(0, (1 << pick()) | (1 if units is None else 1 << int(units[0])), n), 0.5)
+    state = int(rng.integers(0, 1 << min(n, 62)))
+    if units is not None:
+        state |= sum(int(rng.integers(0, 2)) << int(q) for q in units)
+    return from_circuit(0, n, obs, PauliCircuit(layers), state, **kw)

@@ -19,7 +19,7 @@ import math
 import numpy as np
 import pytest
 from adjoint_ref import propagate_with_tangents
-from harness import from_circuit, from_workload, make_cfg
+from harness import from_circuit, from_workload, make_cfg, random_pauli_problem, spread_units
 from test_adjoint_cpu import dense_gradient, random_circuit
 
 import propaq_b200 as pq
@@ -99,8 +99,6 @@ def test_gradient_matches_forward_mode_reference(gpu_engine, oracle, case, seed)
 
 def test_gradient_on_a_wide_register(gpu_engine, oracle):
     # 64-word keys (2048 qubits), 10 active qubits spread over the register.
-    from test_gpu_parity import random_pauli_problem, spread_units
-
     p = random_pauli_problem(4, 2048, n_gates=50, clifford_frac=0.0, units=spread_units(4, 2048, 10), max_weight=4,
                              min_coeff=1e-3)
     e_ref, g_ref = propagate_with_tangents(oracle, p)
