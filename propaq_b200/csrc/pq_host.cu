@@ -874,30 +874,35 @@ int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
 
 // Grid of one sweep launch.  With blocks_per_sm 0 (the default) it follows
 // the live count at the launch: one block per SM while every row has a thread
-// of its own, two per SM up to 2^20 rows, else `max_grid`.  A grid below the
-// largest carries the row count it is chosen for (SweepArgs::grid_rows); the
-// sweep stops before an op that outgrows it and the next launch takes the
-// next size.  Fewer blocks make the grid barrier between ops cheaper (one
-// block per SM took TFIM from 1.95 to 1.74 ms), more blocks keep more rows in
-// flight (the 24-site Majorana run needs them: 35 ms at the largest grid,
-// 76 ms at one block per SM).
+// of its own, two per SM up to 2^20 rows, else `max_grid`; and for 1- and
+// 2-word keys from 2^24 rows on, the sweep built for six resident blocks per
+// SM (sweep_kernel_occ).  A grid below the largest carries the row count it
+// is chosen for (SweepArgs::grid_rows); the sweep stops before an op that
+// outgrows it and the next launch takes the next size.  Fewer blocks make the
+// grid barrier between ops cheaper (one block per SM took TFIM from 1.95 to
+// 1.74 ms), more blocks keep more rows in flight (the 24-site Majorana run
+// needs them: 35 ms at the largest grid, 76 ms at one block per SM).
 struct GridChoice {
   int grid;
   u64 rows;  // 0: no limit
+  bool occ;  // launch sweep_kernel_occ
 };
+constexpr u64 OCC_ROWS = 1ULL << 24;
 GridChoice choose_grid(const Plan& P, const Inputs& in, int max_grid) {
-  if (in.cfg->blocks_per_sm != 0) return {max_grid, 0};
-  const auto tier = [&](int bps) {
+  if (in.cfg->blocks_per_sm != 0) return {max_grid, 0, false};
+  const auto tier = [&](int bps, bool occ) {
     return with_words(P.W, [&](auto w) {
       constexpr int WW = decltype(w)::value;
-      return P.alg == 0 ? pq::sweep_grid<WW, 0>(bps) : pq::sweep_grid<WW, 1>(bps);
+      return P.alg == 0 ? pq::sweep_grid<WW, 0>(bps, occ) : pq::sweep_grid<WW, 1>(bps, occ);
     });
   };
-  const int g1 = tier(1), g2 = tier(2);
+  const int g1 = tier(1, false), g2 = tier(2, false);
   const u64 r1 = (u64)g1 * 256, r2 = 1ULL << 20;
-  if (g1 < max_grid && P.n_live <= r1) return {g1, r1};
-  if (g2 < max_grid && P.n_live <= r2) return {g2, r2};
-  return {max_grid, 0};
+  if (g1 < max_grid && P.n_live <= r1) return {g1, r1, false};
+  if (g2 < max_grid && P.n_live <= r2) return {g2, r2, false};
+  if (P.W > 2) return {max_grid, 0, false};
+  if (P.n_live <= OCC_ROWS) return {max_grid, OCC_ROWS, false};
+  return {tier(0, true), 0, true};
 }
 
 // Runs every built op of one plan, relaunching after capacity growth and when
@@ -923,7 +928,8 @@ int execute_launches(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size
     cudaEventRecord(E->ev_l0, E->stream);
     e = with_words(P.W, [&](auto w) {
       constexpr int WW = decltype(w)::value;
-      return P.alg == 0 ? pq::launch_sweep<WW, 0>(a, grid, E->stream) : pq::launch_sweep<WW, 1>(a, grid, E->stream);
+      return P.alg == 0 ? pq::launch_sweep<WW, 0>(a, grid, E->stream, gc.occ)
+                        : pq::launch_sweep<WW, 1>(a, grid, E->stream, gc.occ);
     });
     if (e != cudaSuccess) return E->cuda_fail(e, "sweep launch");
     cudaEventRecord(E->ev_l1, E->stream);

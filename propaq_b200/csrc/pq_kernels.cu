@@ -1182,6 +1182,17 @@ __global__ void __launch_bounds__(BLOCK, MinBlocks<W>::value) sweep_kernel(const
   sweep_body<W, ALG>(a, Grp{blockIdx.x, gridDim.x});
 }
 
+// The same sweep for 1- and 2-word keys, compiled for six resident blocks of
+// 256 per SM (42 registers a thread) instead of four.  For live sets of
+// 2^24 rows and more, where each op streams the rows from HBM, the extra
+// warps in flight hide more of the random partner lookups (the 32-site
+// Majorana run: 602 -> 562 ms); with fewer rows the registers of
+// sweep_kernel win (the TFIM chain ran 11% slower at six blocks).
+template <int W, int ALG>
+__global__ void __launch_bounds__(BLOCK, 6) sweep_kernel_occ(const SweepArgs a) {
+  sweep_body<W, ALG>(a, Grp{blockIdx.x, gridDim.x});
+}
+
 // A batch: each instance owns the contiguous blocks [blk_begin, blk_begin +
 // blk_count) of the cooperative grid and runs its own op sequence with its own
 // barrier; block_inst maps a block to its instance.  Instances run at WM or
@@ -1518,7 +1529,13 @@ int co_resident_grid(Kernel k, int blocks_per_sm, int* sms, int* per_sm) {
 }
 
 template <int W, int ALG>
-int sweep_grid(int blocks_per_sm) {
+int sweep_grid(int blocks_per_sm, bool occ) {
+  if constexpr (W <= 2) {
+    if (occ) {
+      static int sms = 0, per_sm = 0;
+      return co_resident_grid(sweep_kernel_occ<W, ALG>, blocks_per_sm, &sms, &per_sm);
+    }
+  }
   static int sms = 0, per_sm = 0;
   return co_resident_grid(sweep_kernel<W, ALG>, blocks_per_sm, &sms, &per_sm);
 }
@@ -1530,10 +1547,14 @@ int batch_grid(int blocks_per_sm) {
 }
 
 template <int W, int ALG>
-cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s) {
+cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s, bool occ) {
   SweepArgs args = a;
   void* params[] = {&args};
-  return cudaLaunchCooperativeKernel((const void*)sweep_kernel<W, ALG>, dim3(grid), dim3(BLOCK), params, 0, s);
+  const void* k = (const void*)sweep_kernel<W, ALG>;
+  if constexpr (W <= 2) {
+    if (occ) k = (const void*)sweep_kernel_occ<W, ALG>;
+  }
+  return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(BLOCK), params, 0, s);
 }
 
 template <int W, int ALG>
@@ -1605,9 +1626,9 @@ cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const
 }
 
 #define PQ_INSTANTIATE(Wv, Av)                                                                          \
-  template int sweep_grid<Wv, Av>(int);                                                                    \
+  template int sweep_grid<Wv, Av>(int, bool);                                                              \
   template int batch_grid<Wv, Av>(int);                                                                    \
-  template cudaError_t launch_sweep<Wv, Av>(const SweepArgs&, int, cudaStream_t);                       \
+  template cudaError_t launch_sweep<Wv, Av>(const SweepArgs&, int, cudaStream_t, bool);                 \
   template cudaError_t launch_batch_sweep<Wv, Av>(const SweepArgs*, const u32*, int, cudaStream_t);     \
   template cudaError_t launch_adjoint<Wv, Av>(const AdjointArgs&, int, cudaStream_t);                   \
   template cudaError_t launch_adjoint_seed<Wv, Av>(const ExpectArgs&, const u64*, u64, double*, cudaStream_t); \

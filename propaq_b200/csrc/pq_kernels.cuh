@@ -151,12 +151,14 @@ struct ExpectPartial {
 };
 
 // Co-resident grid of the sweep kernel for this W / algebra: every SM with
-// blocks_per_sm blocks (0 or more than fit = as many as fit).
+// blocks_per_sm blocks (0 or more than fit = as many as fit).  occ selects,
+// for 1- and 2-word keys, the build of the sweep for six resident blocks per
+// SM (for live sets of 2^24 rows and more); wider keys ignore it.
 template <int W, int ALG>
-int sweep_grid(int blocks_per_sm);
+int sweep_grid(int blocks_per_sm, bool occ = false);
 
 template <int W, int ALG>
-cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s, bool occ = false);
 // Batched sweep of instances with keys WM or WM / 2 words wide (n_words):
 // args[i] describes instance i and its blk_begin / blk_count slice of the
 // grid; block_inst[b] is the instance of block b.  batch_grid is its

@@ -407,6 +407,23 @@ def test_grid_follows_the_live_count(gpu_engine, oracle, make):
     assert ok
 
 
+def test_six_block_build_on_a_large_live_set(gpu_engine):
+    # Config 3 (32 sites, 99M live rows): past 2^24 rows the default grid
+    # switches to the sweep built for six resident blocks per SM.  A fixed
+    # grid (four blocks per SM, never that build) must give the same live
+    # count after every gate and the same expectation value.
+    p = from_workload(workloads.majorana_givens())
+    cfg, keep = make_cfg(p, want_terms=False)
+    auto, nt_auto = gpu_engine.run(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag)
+    cfg.blocks_per_sm = 4
+    fixed, nt_fixed = gpu_engine.run(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag)
+    assert auto.peak_terms > 1 << 24
+    assert auto.sweep_launches > fixed.sweep_launches
+    assert np.array_equal(nt_auto, nt_fixed)
+    assert auto.terms_below_cutoff == fixed.terms_below_cutoff
+    assert abs(auto.expectation_value - fixed.expectation_value) <= 1e-13 * max(1.0, abs(fixed.expectation_value))
+
+
 def test_width_errors(gpu_engine):
     big = PauliTermSum({PauliString(0, 1, 2049): 1.0})
     with pytest.raises(ValueError, match="exceeds the engine's maximum of 2048"):
