@@ -713,10 +713,15 @@ def main():
                 clocks=clocks, peak_terms=peak, expectation_value=r.expectation_value)
     line["config"]["parallelism"] = f"replicas x{world}"
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, runs, el, _ = run_cpu_baseline(builder, args.cpu_seconds, cores)
+        v, runs, el, ores = run_cpu_baseline(builder, args.cpu_seconds, cores)
         line["cpu_baseline"] = {"value": v, "unit": "terms/s", "cores": cores, "kind": "port",
                                 "sample": f"{runs} whole run(s) of the workload in {el:.1f} s, oracle with "
                                           f"{cores} partitions/threads"}
+        # the same run's answer from the oracle, with the plain relative error
+        # of the engine's expectation value against it
+        ref = ores.expectation_accurate
+        line["oracle_expectation_value"] = ref
+        line["rel_err_vs_oracle"] = abs(r.expectation_value - ref) / abs(ref) if ref else abs(r.expectation_value)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

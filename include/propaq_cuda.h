@@ -85,6 +85,9 @@ typedef struct pq_run_config {
                                 every row has a thread, 2 up to 2^20 rows, then
                                 as many as fit (a launch stops and is relaunched
                                 when its live count outgrows its grid)          */
+  uint32_t log_gates;        /* keep per-gate records for pq_result_gates (the
+                                Logger's verbose log); rotations then run one op
+                                each, unfused, so each has its own device time  */
 } pq_run_config;
 
 /* crates/core/src/interface/results.rs:8-51 (PropagationResult), plus the
@@ -123,6 +126,32 @@ int pq_engine_create(pq_engine** out, int device);
 void pq_engine_destroy(pq_engine* engine);
 const char* pq_engine_last_error(const pq_engine* engine);
 
+/* Limits of one engine; a zero field keeps its default.  The reference's
+ * counterparts are fixed: its term index ceiling
+ * (crates/core/src/storage/operator_index.rs:116-127, TermIndexCeilingReached
+ * -> RuntimeError) and the host's allocator.  Here a caller may lower the
+ * ceiling and give the engine a device-memory budget; a run that needs more
+ * fails with PQ_ERR_CEILING / PQ_ERR_OOM and the engine stays usable.  The
+ * wait limits bound the device's grid barrier and look-back spins (a wait
+ * that runs out ends the launch with PQ_ERR_DEVICE_TIMEOUT instead of
+ * hanging); hold_block / hold_us exist for tests of that path: one block of
+ * every sweep launch waits hold_us microseconds (at most 100 ms) before its
+ * first op, so that short wait limits run out. */
+typedef struct pq_engine_limits {
+  uint64_t max_rows;         /* live-term ceiling (rounded down to a power of two);
+                                0 = 2^31, the table's row index                 */
+  uint64_t max_device_bytes; /* device memory the engine's buffers may hold; 0 = any */
+  uint32_t barrier_spins;    /* polls of a grid-barrier wait; 0 = 2^25 (~2 s)   */
+  uint32_t lookback_spins;   /* polls of a tile look-back wait; 0 = 2^22 (~0.3 s) */
+  uint32_t hold_block;       /* block (of a launch, or of a batch instance's slice) */
+  uint32_t hold_us;          /* that waits before its first op; 0 = none        */
+} pq_engine_limits;
+/* NULL restores every default.  Applies to the engine's later runs. */
+int pq_engine_set_limits(pq_engine* engine, const pq_engine_limits* limits);
+/* Device bytes the engine holds in buffers allocated since its limits were
+ * last set (what max_device_bytes is compared with). */
+uint64_t pq_engine_device_bytes(const pq_engine* engine);
+
 /* Runs one propagation; replaces engine::run / run_at_width
  * (crates/pauli/src/engine.rs:74-238, :305-357; crates/majorana/src/engine.rs).
  *
@@ -148,6 +177,29 @@ int pq_run(pq_engine* engine, const pq_run_config* cfg, const uint64_t* obs_word
  * (crates/pauli/src/engine.rs:216-224, partitioned_termsum.rs:265-272).
  * Writes min(cap, n) terms, returns n. */
 size_t pq_result_terms(pq_engine* engine, uint64_t* keys, double* coeffs, size_t cap);
+
+/* One gate's record of the last pq_run made with log_gates: the reference's
+ * GateRecord (crates/pauli/src/engine.rs:252-265, written to the verbose log
+ * by crates/pauli/src/propagator.rs:23-73) with the device's time. */
+typedef struct pq_gate_record {
+  uint64_t terms_before, terms_after; /* live terms around the gate             */
+  uint64_t terms_gained;              /* rows the gate created                  */
+  uint64_t declined;                  /* sin branches the emit check held back  */
+  uint64_t emitted;                   /* sin branches that went out             */
+  uint64_t exchange_hits;             /* ... onto a row that was already live   */
+  double discarded_coeff_l1;          /* sum of |held branch| that no partner
+                                         claimed (termsum.rs:604-628)          */
+  double discarded_coeff_max;         /* largest of those                       */
+  double elapsed_ms;                  /* device time of the gate's op; 0 for a
+                                         rotation deferred into the Clifford frame */
+  uint32_t layer_idx;                 /* layer in Heisenberg order              */
+  int32_t op;                         /* the gate's op in the sweep; -1 = deferred */
+} pq_gate_record;
+
+/* Per-gate records of the last pq_run made with log_gates, gates in
+ * Heisenberg order.  Writes min(cap, n) records, returns n (0 without
+ * log_gates). */
+size_t pq_result_gates(pq_engine* engine, pq_gate_record* out, size_t cap);
 
 /* One propagation of a batch: the arguments of pq_run in one record.  Keys
  * are pq_words_for_units(cfg.n_units) words wide. */
@@ -270,11 +322,16 @@ int pq_plugin_truncator_keep(const pq_plugin* plugin, uint32_t basis_kind, const
  * sums) must fit; larger inputs are refused with PQ_ERR_INVALID and a message
  * in `err`.  n_units <= 256.
  *
- * The first call on a device resolves the array's address on that device
- * (the current device); make that first call before any stream capture.
- * Every call shares the array: calls that overlap on one device race, so
- * serialise them.  Runs on the legacy default stream and returns when the
- * value has been copied to *out_value. */
+ * Every call looks the array's address up in the current context (a
+ * cudaGetSymbolAddress, which allocates nothing), so it stays right after a
+ * cudaDeviceReset and in a context the caller created.  The array is
+ * committed when the library's module is loaded on a device: at the first
+ * call there (at library load under CUDA_MODULE_LOADING=EAGER, on every
+ * device).  Make that first call before the program reserves its device
+ * memory, and before any stream capture.  Every call shares the array, which
+ * keeps the last call's contents: calls that overlap on one device race, so
+ * serialise them.  n_terms = 0 gives 0.  Runs on the legacy default stream
+ * and returns when the value has been copied to *out_value. */
 #define PQ_NOALLOC_SCRATCH_BYTES (16u << 20)
 int pq_expectation_noalloc(uint32_t basis_kind, uint32_t n_units, const uint64_t* keys,
                            const double* coeffs, size_t n_terms, const uint64_t* diag_state,

@@ -8,7 +8,13 @@ set -e
 REF=${PROPAQ_REFERENCE:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
-[ -d "$REF/examples/plugins/c" ] || { echo "reference tree not found at $REF" >&2; exit 1; }
+# Without the reference tree (the GPU box has only the prebuilt fixtures)
+# there is nothing to build: --if-present makes that a quiet no-op.
+if [ ! -d "$REF/examples/plugins/c" ]; then
+  [ "$1" = "--if-present" ] && exit 0
+  echo "reference tree not found at $REF" >&2
+  exit 1
+fi
 mkdir -p "$OUT"
 for src in "$REF"/examples/plugins/c/noise/*.c "$REF"/examples/plugins/c/truncation/*.c; do
   name=$(basename "$src" .c)

@@ -50,6 +50,25 @@ class RunConfig(ctypes.Structure):
         ("noise_plugin", ctypes.c_void_p),
         ("want_terms", ctypes.c_uint32),
         ("blocks_per_sm", ctypes.c_uint32),
+        ("log_gates", ctypes.c_uint32),
+    ]
+
+
+class GateRecord(ctypes.Structure):
+    """pq_gate_record: one gate of a logged run (the reference's GateRecord)."""
+
+    _fields_ = [
+        ("terms_before", ctypes.c_uint64),
+        ("terms_after", ctypes.c_uint64),
+        ("terms_gained", ctypes.c_uint64),
+        ("declined", ctypes.c_uint64),
+        ("emitted", ctypes.c_uint64),
+        ("exchange_hits", ctypes.c_uint64),
+        ("discarded_coeff_l1", ctypes.c_double),
+        ("discarded_coeff_max", ctypes.c_double),
+        ("elapsed_ms", ctypes.c_double),
+        ("layer_idx", ctypes.c_uint32),
+        ("op", ctypes.c_int32),
     ]
 
 
@@ -105,6 +124,14 @@ class Instance(ctypes.Structure):
     ]
 
 
+class EngineLimits(ctypes.Structure):
+    """pq_engine_limits."""
+
+    _fields_ = [("max_rows", ctypes.c_uint64), ("max_device_bytes", ctypes.c_uint64),
+                ("barrier_spins", ctypes.c_uint32), ("lookback_spins", ctypes.c_uint32),
+                ("hold_block", ctypes.c_uint32), ("hold_us", ctypes.c_uint32)]
+
+
 class BatchTuning(ctypes.Structure):
     """pq_batch_tuning."""
 
@@ -120,9 +147,12 @@ _SIGNATURES = {
     "pq_engine_create": (ctypes.c_int, [ctypes.POINTER(_V), ctypes.c_int]),
     "pq_engine_destroy": (None, [_V]),
     "pq_engine_last_error": (ctypes.c_char_p, [_V]),
+    "pq_engine_set_limits": (ctypes.c_int, [_V, ctypes.POINTER(EngineLimits)]),
+    "pq_engine_device_bytes": (ctypes.c_uint64, [_V]),
     "pq_run": (ctypes.c_int, [_V, ctypes.POINTER(RunConfig), _V, _V, _Z, _V, _V, _Z, _V, _Z, _V, _Z, _V,
                               ctypes.POINTER(RunResult)]),
     "pq_result_terms": (_Z, [_V, _V, _V, _Z]),
+    "pq_result_gates": (_Z, [_V, _V, _Z]),
     "pq_run_batch": (ctypes.c_int, [_V, ctypes.POINTER(Instance), _Z, ctypes.POINTER(BatchTuning)]),
     "pq_result_terms_at": (_Z, [_V, _Z, _V, _V, _Z]),
     "pq_run_adjoint": (ctypes.c_int, [_V, ctypes.POINTER(RunConfig), _V, _V, _Z, _V, _V, _Z, _V, _Z, _V, _Z, _U32,
@@ -190,6 +220,20 @@ class Engine:
         if h and _lib is not None:
             _lib.pq_engine_destroy(h)
             self._h = None
+
+    def set_limits(self, max_rows: int = 0, max_device_bytes: int = 0, barrier_spins: int = 0,
+                   lookback_spins: int = 0, hold_block: int = 0, hold_us: int = 0):
+        """pq_engine_set_limits; no arguments restore every default."""
+        lim = EngineLimits(max_rows, max_device_bytes, barrier_spins, lookback_spins, hold_block, hold_us)
+        with self.lock:
+            rc = lib().pq_engine_set_limits(self._h, ctypes.byref(lim))
+        if rc != PQ_OK:
+            raise_for(rc, "pq_engine_set_limits failed")
+
+    def device_bytes(self) -> int:
+        """Device bytes held in buffers allocated since the limits were last set."""
+        with self.lock:
+            return int(lib().pq_engine_device_bytes(self._h))
 
     def run(self, cfg: RunConfig, obs_words, obs_coeffs, gate_words, gate_angles, layer_offsets,
             diag_state=None, want_n_terms=True):
@@ -266,6 +310,15 @@ class Engine:
             rc = lib().pq_run_batch(self._h, insts, len(items), ctypes.byref(tune))
             if rc != PQ_OK:
                 raise_for(rc, lib().pq_engine_last_error(self._h).decode(errors="replace"))
+        return out
+
+    def gates(self):
+        """Per-gate records (GateRecord array) of the last run made with log_gates."""
+        with self.lock:
+            n = lib().pq_result_gates(self._h, None, 0)
+            out = (GateRecord * n)()
+            if n:
+                lib().pq_result_gates(self._h, out, n)
         return out
 
     def terms(self, n_words: int, index: int = 0):

@@ -58,6 +58,7 @@ class _Circuit:
         """Reversed order and negated angles (U dagger), compound gates kept in order
         (propaq/circuits/_utils.py: compound_gate_reversed)."""
         out = type(self).__new__(type(self))
+        out.__dict__.update(self.__dict__)
         out._layers = [_compound_reversed(layer) for layer in reversed(self._layers)]
         return out
 
@@ -84,7 +85,14 @@ class PauliCircuit(_Circuit):
 
 
 class MajoranaCircuit(_Circuit):
+    """Layers of Majorana rotations; `n_modes` as the reference's constructor
+    takes it (propaq/circuits/majorana/circuit.py:35-47), optional here."""
+
     _rotation_cls = MajoranaRotation
+
+    def __init__(self, rotations_or_layers, n_modes: int | None = None):
+        super().__init__(rotations_or_layers)
+        self.n_modes = n_modes
 
 
 # ---------------------------------------------------------------- Pauli gates

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 namespace pq {
 
@@ -57,6 +58,32 @@ struct GenInfo {
   int aux;       // Pauli: Y sites of the generator; Majorana: its length
   double sign;   // +1 / -1 carried by the generator from the frame
 };
+
+// GenInfo of generator g (W words, already conjugated through the frame) with
+// frame sign `sign`; built once per rotation on the host.
+template <int W>
+inline GenInfo<W> make_gen_info(int alg, const u64* g, int sign) {
+  auto pc = [](u64 x) { return __builtin_popcountll(x); };
+  GenInfo<W> gi;
+  int aux = 0;
+  for (int i = 0; i < W; ++i) {
+    gi.gen[i] = g[i];
+    gi.fold[i] = alg == 0 ? (((g[i] & EVEN) << 1) | ((g[i] >> 1) & EVEN)) : g[i];
+    aux += alg == 0 ? pc(g[i] & (g[i] >> 1) & EVEN) : pc(g[i]);
+  }
+  gi.aux = aux;
+  gi.sign = sign < 0 ? -1.0 : 1.0;
+  gi.carry = 0;
+  int above = 0;
+  for (int i = W - 1; i >= 0; --i) {
+    u64 s = g[i] >> 1;
+    for (int sh = 1; sh < 64; sh <<= 1) s ^= s >> sh;
+    gi.sfx[i] = s;
+    if (above) gi.carry |= 1ull << i;
+    above ^= pc(g[i]) & 1;
+  }
+  return gi;
+}
 
 // ---------------------------------------------------------------- Pauli
 // crates/pauli/src/algebra.rs:130-240

@@ -137,6 +137,50 @@ u64 next_pow2(u64 x) {
 
 }  // namespace
 
+// Device allocations of an engine, counted against its budget
+// (pq_engine_limits::max_device_bytes).  The entry points that act on an
+// engine point t_budget at its budget for the duration of the call, so the
+// helpers below need no engine argument; allocations made with no budget in
+// force (or before a limit was set) are not counted.
+struct MemBudget {
+  size_t limit = 0, used = 0;  // limit 0 = none
+  std::unordered_map<void*, size_t> sizes;
+};
+thread_local MemBudget* t_budget = nullptr;
+
+struct BudgetScope {
+  MemBudget* saved;
+  explicit BudgetScope(MemBudget* b) : saved(t_budget) { t_budget = b; }
+  ~BudgetScope() { t_budget = saved; }
+};
+
+template <class T>
+cudaError_t dmalloc(T** p, size_t n) {
+  *p = nullptr;
+  MemBudget* b = t_budget;
+  if (b && b->limit && b->used + n > b->limit) return cudaErrorMemoryAllocation;
+  void* q = nullptr;
+  const cudaError_t e = cudaMalloc(&q, n);
+  if (e != cudaSuccess) return e;
+  *p = static_cast<T*>(q);
+  if (b) {
+    b->used += n;
+    b->sizes[q] = n;
+  }
+  return cudaSuccess;
+}
+inline void dfree(void* p) {
+  if (!p) return;
+  if (MemBudget* b = t_budget) {
+    const auto it = b->sizes.find(p);
+    if (it != b->sizes.end()) {
+      b->used -= it->second;
+      b->sizes.erase(it);
+    }
+  }
+  cudaFree(p);
+}
+
 // ---------------------------------------------------------------- engine
 namespace {
 
@@ -172,6 +216,8 @@ struct Slot {
   u64* hist = nullptr;
   u64* anti = nullptr;
   u64* stamps = nullptr;
+  u64* logs = nullptr;  // per-op emit statistics of a logged run (LOG_WORDS per op)
+  std::vector<pq_gate_record> gate_log;  // per-gate records of the last logged run
   void* d_gates = nullptr;
   size_t gates_bytes = 0;
   double* d_tables = nullptr;
@@ -190,23 +236,23 @@ struct Slot {
 
   void free_rows() {
     for (int i = 0; i < 2; ++i) {
-      if (keys[i]) cudaFree(keys[i]);
-      if (coeffs[i]) cudaFree(coeffs[i]);
+      if (keys[i]) dfree(keys[i]);
+      if (coeffs[i]) dfree(coeffs[i]);
       keys[i] = nullptr;
       coeffs[i] = nullptr;
     }
-    if (table) cudaFree(table);
-    if (status) cudaFree(status);
+    if (table) dfree(table);
+    if (status) dfree(status);
     table = nullptr;
     status = nullptr;
     cap = tcap = 0;
   }
   void free_ops() {
-    for (void* p : {(void*)d_ops, (void*)tickets, (void*)hist, (void*)anti, (void*)stamps})
-      if (p) cudaFree(p);
+    for (void* p : {(void*)d_ops, (void*)tickets, (void*)hist, (void*)anti, (void*)stamps, (void*)logs})
+      if (p) dfree(p);
     d_ops = nullptr;
     tickets = nullptr;
-    hist = anti = stamps = nullptr;
+    hist = anti = stamps = logs = nullptr;
     ops_cap = 0;
   }
   void free_all() {
@@ -214,7 +260,7 @@ struct Slot {
     free_ops();
     for (void* p : {(void*)d_gates, (void*)d_tables, (void*)partials, (void*)frame_img, (void*)frame_sgn,
                     (void*)host_state, (void*)host_factor, (void*)host_keep})
-      if (p) cudaFree(p);
+      if (p) dfree(p);
     host_state = nullptr;
     host_factor = nullptr;
     host_keep = nullptr;
@@ -233,12 +279,12 @@ struct Slot {
 template <class T>
 cudaError_t grow_pair(T** dev, T** host, size_t* cap, size_t n) {
   if (*cap >= n) return cudaSuccess;
-  if (*dev) cudaFree(*dev);
+  if (*dev) dfree(*dev);
   if (host && *host) cudaFreeHost(*host);
   *dev = nullptr;
   if (host) *host = nullptr;
   *cap = 0;
-  cudaError_t e = cudaMalloc(dev, n * sizeof(T));
+  cudaError_t e = dmalloc(dev, n * sizeof(T));
   if (e == cudaSuccess && host) e = cudaMallocHost(host, n * sizeof(T));
   if (e == cudaSuccess) *cap = n;
   return e;
@@ -254,7 +300,7 @@ struct DevBuf {
   cudaError_t ensure(size_t n) {
     if (bytes >= n) return cudaSuccess;
     release();
-    const cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1));
+    const cudaError_t e = dmalloc(&p, std::max<size_t>(n, 1));
     if (e != cudaSuccess) {
       p = nullptr;
       return e;
@@ -263,7 +309,7 @@ struct DevBuf {
     return cudaSuccess;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) dfree(p);
     p = nullptr;
     bytes = 0;
   }
@@ -300,6 +346,30 @@ struct pq_engine {
   DevBuf g_pool, g_lam, g_ops;
   std::vector<DevBuf> g_ck;
   size_t g_need = 0;
+  // pq_engine_set_limits: the row ceiling, the device-memory budget the
+  // engine's allocations count against, the device wait limits and the
+  // failure tests' hold.
+  pq_engine_limits lim{};
+  MemBudget budget;
+
+  // Largest row capacity a run may use: a power of two (the table is 2x the
+  // rows and is indexed by mask), at most MAX_ROWS.
+  u64 row_ceiling() const {
+    const u64 m = lim.max_rows ? std::min<u64>(lim.max_rows, MAX_ROWS) : MAX_ROWS;
+    u64 p = 1;
+    while (2 * p <= m) p *= 2;
+    return p;
+  }
+  void init_waits(pq::SweepState& st) const {
+    st.barrier_limit = lim.barrier_spins ? lim.barrier_spins : pq::DEFAULT_BARRIER_POLLS;
+    st.lookback_limit = lim.lookback_spins ? lim.lookback_spins : pq::DEFAULT_LOOKBACK_POLLS;
+  }
+  // The limits' share of a sweep launch's arguments.
+  void limit_args(pq::SweepArgs& a) const {
+    a.cap = std::min<u64>(a.cap, row_ceiling());
+    a.hold_block = lim.hold_block;
+    a.hold_us = std::min<u32>(lim.hold_us, 100000);
+  }
 
   int fail(int code, const std::string& m) {
     err = m;
@@ -316,7 +386,7 @@ struct pq_engine {
     for (DevBuf* b : {&g_pool, &g_lam, &g_ops}) b->release();
     for (DevBuf& b : g_ck) b.release();
     for (void* p : {(void*)d_states, (void*)d_args, (void*)d_block_inst, (void*)d_err, (void*)d_idle})
-      if (p) cudaFree(p);
+      if (p) dfree(p);
     for (void* p : {(void*)h_states, (void*)h_args, (void*)h_block_inst})
       if (p) cudaFreeHost(p);
     for (auto ev : {ev_begin, ev_end, ev_l0, ev_l1})
@@ -347,20 +417,20 @@ struct pq_engine {
     const u64 n_status = new_cap / TILE_ROWS + 2;
     auto cleanup = [&]() {
       for (int i = 0; i < 2; ++i) {
-        if (nk[i]) cudaFree(nk[i]);
-        if (nc[i]) cudaFree(nc[i]);
+        if (nk[i]) dfree(nk[i]);
+        if (nc[i]) dfree(nc[i]);
       }
-      if (nt) cudaFree(nt);
-      if (ns) cudaFree(ns);
+      if (nt) dfree(nt);
+      if (ns) dfree(ns);
     };
     for (int i = 0; i < 2; ++i) {
-      if ((e = cudaMalloc(&nk[i], new_cap * Wn * 8)) != cudaSuccess ||
-          (e = cudaMalloc(&nc[i], new_cap * 8)) != cudaSuccess) {
+      if ((e = dmalloc(&nk[i], new_cap * Wn * 8)) != cudaSuccess ||
+          (e = dmalloc(&nc[i], new_cap * 8)) != cudaSuccess) {
         cleanup();
         return cuda_fail(e, "allocating term rows");
       }
     }
-    if ((e = cudaMalloc(&nt, ntcap * 8)) != cudaSuccess || (e = cudaMalloc(&ns, n_status * 8)) != cudaSuccess) {
+    if ((e = dmalloc(&nt, ntcap * 8)) != cudaSuccess || (e = dmalloc(&ns, n_status * 8)) != cudaSuccess) {
       cleanup();
       return cuda_fail(e, "allocating the hash table");
     }
@@ -399,10 +469,11 @@ struct pq_engine {
     if (S.ops_cap >= n_ops) return PQ_OK;
     S.free_ops();
     cudaError_t e;
-    if ((e = cudaMalloc(&S.d_ops, n_ops * sizeof(pq::OpDesc))) != cudaSuccess ||
-        (e = cudaMalloc(&S.tickets, n_ops * 4)) != cudaSuccess ||
-        (e = cudaMalloc(&S.hist, n_ops * 8)) != cudaSuccess || (e = cudaMalloc(&S.anti, n_ops * 8)) != cudaSuccess ||
-        (e = cudaMalloc(&S.stamps, n_ops * 8)) != cudaSuccess)
+    if ((e = dmalloc(&S.d_ops, n_ops * sizeof(pq::OpDesc))) != cudaSuccess ||
+        (e = dmalloc(&S.tickets, n_ops * 4)) != cudaSuccess ||
+        (e = dmalloc(&S.hist, n_ops * 8)) != cudaSuccess || (e = dmalloc(&S.anti, n_ops * 8)) != cudaSuccess ||
+        (e = dmalloc(&S.stamps, n_ops * 8)) != cudaSuccess ||
+        (e = dmalloc(&S.logs, n_ops * pq::LOG_WORDS * 8)) != cudaSuccess)
       return cuda_fail(e, "allocating op arrays");
     S.ops_cap = n_ops;
     return PQ_OK;
@@ -413,25 +484,7 @@ namespace {
 
 template <int W>
 pq::GenInfo<W> make_gen(int alg, const u64* g, int sign) {
-  pq::GenInfo<W> gi;
-  int aux = 0;
-  for (int i = 0; i < W; ++i) {
-    gi.gen[i] = g[i];
-    gi.fold[i] = alg == 0 ? (((g[i] & EVEN) << 1) | ((g[i] >> 1) & EVEN)) : g[i];
-    aux += alg == 0 ? hpopc(g[i] & (g[i] >> 1) & EVEN) : hpopc(g[i]);
-  }
-  gi.aux = aux;
-  gi.sign = sign < 0 ? -1.0 : 1.0;
-  gi.carry = 0;
-  int above = 0;
-  for (int i = W - 1; i >= 0; --i) {
-    u64 s = g[i] >> 1;
-    for (int sh = 1; sh < 64; sh <<= 1) s ^= s >> sh;
-    gi.sfx[i] = s;
-    if (above) gi.carry |= 1ull << i;
-    above ^= hpopc(g[i]) & 1;
-  }
-  return gi;
+  return pq::make_gen_info<W>(alg, g, sign);
 }
 
 // One propagation's inputs as the C ABI receives them; keys are `in_words`
@@ -476,6 +529,7 @@ struct Plan {
   const Plugin* keynoise = nullptr;
   bool host_ops = false;
   bool defer = true;
+  bool log = false;  // per-gate records for the verbose log (pq_run_config::log_gates)
   std::vector<u64> hk;
   std::vector<double> hc;
   u64 n0 = 0;
@@ -518,6 +572,7 @@ int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
   P.has_c = cfg->has_min_coeff != 0;
   P.ccut = cfg->min_coeff;
   P.has_floor = cfg->min_terms >= 0;
+  P.log = cfg->log_gates != 0;
   P.floor_terms = P.has_floor ? (u64)cfg->min_terms : 0;
   const Plugin* np = reinterpret_cast<const Plugin*>(cfg->noise_plugin);
   P.tlen = cfg->noise_table_len ? cfg->noise_table_len : (size_t)P.n_units + 1;
@@ -616,10 +671,10 @@ int setup_slot(pq_engine* E, Slot& S, Plan& P) {
   if (int rc = E->ensure_ops(S, n_ops_max)) return rc;
   const size_t gbytes = std::max<size_t>(P.in->n_gates, 1) * gdesc_words(W) * 8;
   if (S.gates_bytes < gbytes) {
-    if (S.d_gates) cudaFree(S.d_gates);
+    if (S.d_gates) dfree(S.d_gates);
     S.d_gates = nullptr;
     S.gates_bytes = 0;
-    if ((e = cudaMalloc(&S.d_gates, gbytes)) != cudaSuccess) return E->cuda_fail(e, "gate descriptors");
+    if ((e = dmalloc(&S.d_gates, gbytes)) != cudaSuccess) return E->cuda_fail(e, "gate descriptors");
     S.gates_bytes = gbytes;
   }
   if (!P.tables.empty()) {
@@ -628,10 +683,11 @@ int setup_slot(pq_engine* E, Slot& S, Plan& P) {
     cudaMemcpyAsync(S.d_tables, P.tables.data(), P.tables.size() * 8, cudaMemcpyHostToDevice, E->stream);
   }
   if (!S.partials) {
-    if ((e = cudaMalloc(&S.partials, sizeof(pq::ExpectPartial) * E->expect_grid)) != cudaSuccess)
+    if ((e = dmalloc(&S.partials, sizeof(pq::ExpectPartial) * E->expect_grid)) != cudaSuccess)
       return E->cuda_fail(e, "partials");
   }
   cudaMemsetAsync(S.anti, 0, n_ops_max * 8, E->stream);
+  if (P.log) cudaMemsetAsync(S.logs, 0, n_ops_max * pq::LOG_WORDS * 8, E->stream);
   if (S.epoch_base > (1u << 29)) {  // keep status tags unique: restart the epochs on a cleared array
     S.epoch_base = 1;
     cudaMemsetAsync(S.status, 0, (S.cap / TILE_ROWS + 2) * 8, E->stream);
@@ -716,7 +772,7 @@ int build_ops(Plan& P, NeedN need_n) {
 // needs its own record).
 constexpr size_t FUSE_MAX = 2;
 void fuse_groups(Plan& P) {
-  if (P.has_floor || P.host_ops) return;
+  if (P.has_floor || P.host_ops || P.log) return;
   const size_t gw = gdesc_words(P.W);
   const int W = P.W;
   auto gen = [&](size_t op) { return &P.gdesc[P.ops[op].idx * gw]; };  // GateDesc starts with the generator
@@ -825,14 +881,16 @@ pq::SweepArgs sweep_args(Slot& S, const Plan& P, pq::SweepState* st, u32 blk_beg
   a.hist = S.hist;
   a.anti = S.anti;
   a.stamps = S.stamps;
+  a.log = P.log ? S.logs : nullptr;
   a.st = st;
   a.blk_begin = blk_begin;
   a.blk_count = blk_count;
   return a;
 }
 
-pq::SweepState fresh_state(const Plan& P) {
+pq::SweepState fresh_state(const pq_engine* E, const Plan& P) {
   pq::SweepState s{};
+  E->init_waits(s);
   s.n[P.done & 1] = P.n_live;
   s.peak = P.peak;
   s.halt = pq::NOT_HALTED;
@@ -845,13 +903,16 @@ pq::SweepState fresh_state(const Plan& P) {
 // Reads a plan's sweep state after a launch; on a capacity halt grows its rows
 // (the gate at `done` needs 2 N rows) so that the next launch resumes there.
 int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
+  // The launch tagged its tile statuses with epochs from epoch_base; the next
+  // launch must use fresh ones even when this one failed part way, or it
+  // could read this launch's statuses as its own.
+  S.epoch_base += (u32)P.ops.size() + 1;
   if (h.error & pq::ERR_BARRIER_TIMEOUT)
     return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a grid barrier wait expired on the device");
   if (h.error & pq::ERR_LOOKBACK_TIMEOUT)
     return E->fail(PQ_ERR_DEVICE_TIMEOUT, "a tile's look-back wait expired on the device");
   if (h.error) return E->fail(PQ_ERR_CUDA, "device reported error bits " + std::to_string(h.error));
   S.cur = (int)h.cur;
-  S.epoch_base += (u32)P.ops.size() + 1;
   P.done = h.end_op;
   P.n_live = h.n[P.done & 1];
   P.peak = std::max(P.peak, h.peak);
@@ -860,11 +921,12 @@ int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
   P.rec_full = h.rec_full;
   ++P.sweep_launches;
   if (h.halt != pq::NOT_HALTED && !h.grid_stop) {
-    u64 ncap = next_pow2(std::max<u64>(4 * P.n_live, 2 * S.cap));
-    if (ncap > MAX_ROWS) ncap = MAX_ROWS;
+    u64 ncap = next_pow2(std::max<u64>(4 * P.n_live, 2 * std::min(S.cap, E->row_ceiling())));
+    if (ncap > E->row_ceiling()) ncap = E->row_ceiling();
     if (2 * P.n_live > ncap)
       return E->fail(PQ_ERR_CEILING, "term index ceiling reached: " + std::to_string(2 * P.n_live) +
                                          " rows would exceed the engine's capacity");
+    if (ncap <= S.cap) return PQ_OK;  // the ceiling was below the buffers: they already hold ncap rows
     int rc = E->resize(S, ncap, P.n_live, S.cur, P.W);
     if (rc == PQ_ERR_OOM) rc = E->resize(S, next_pow2(2 * P.n_live), P.n_live, S.cur, P.W);
     if (rc) return rc;
@@ -916,11 +978,12 @@ int execute_launches(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size
   while (P.done < end) {
     const GridChoice gc = choose_grid(P, *P.in, max_grid);
     grid = gc.grid;
-    E->h_states[0] = fresh_state(P);
+    E->h_states[0] = fresh_state(E, P);
     cudaMemcpyAsync(E->d_states, E->h_states, sizeof(pq::SweepState), cudaMemcpyHostToDevice, E->stream);
     cudaMemsetAsync(S.tickets + P.done, 0, (end - P.done) * 4, E->stream);
     pq::SweepArgs a = sweep_args(S, P, E->d_states, 0, (u32)grid, end, rec, host);
     a.grid_rows = gc.rows;
+    E->limit_args(a);
     if (!*began) {  // device time starts at the first sweep
       cudaEventRecord(E->ev_begin, E->stream);
       *began = true;
@@ -976,14 +1039,14 @@ int host_decide(pq_engine* E, Slot& S, Plan& P, size_t k, HostOps* ho) {
   cudaError_t e;
   if (S.host_cap < N) {
     for (void* p : {(void*)S.host_state, (void*)S.host_factor, (void*)S.host_keep})
-      if (p) cudaFree(p);
+      if (p) dfree(p);
     S.host_state = nullptr;
     S.host_factor = nullptr;
     S.host_keep = nullptr;
     S.host_cap = 0;
     const size_t cap = std::max<size_t>(N, S.cap);
-    if ((e = cudaMalloc(&S.host_state, cap)) != cudaSuccess || (e = cudaMalloc(&S.host_factor, cap * 8)) != cudaSuccess ||
-        (e = cudaMalloc(&S.host_keep, cap)) != cudaSuccess)
+    if ((e = dmalloc(&S.host_state, cap)) != cudaSuccess || (e = dmalloc(&S.host_factor, cap * 8)) != cudaSuccess ||
+        (e = dmalloc(&S.host_keep, cap)) != cudaSuccess)
       return E->cuda_fail(e, "host decision buffers");
     S.host_cap = cap;
   }
@@ -1124,13 +1187,13 @@ int finalize(pq_engine* E, Slot& S, Plan& P, std::vector<pq::ExpectPartial>* par
   if (!P.frame.identity) {
     const size_t ni = P.frame.rd_img.size(), ns = P.frame.rd_sign.size();
     if (S.frame_cap < ni) {
-      if (S.frame_img) cudaFree(S.frame_img);
-      if (S.frame_sgn) cudaFree(S.frame_sgn);
+      if (S.frame_img) dfree(S.frame_img);
+      if (S.frame_sgn) dfree(S.frame_sgn);
       S.frame_img = nullptr;
       S.frame_sgn = nullptr;
       S.frame_cap = 0;
-      if ((e = cudaMalloc(&S.frame_img, ni * 8)) != cudaSuccess) return E->cuda_fail(e, "frame");
-      if ((e = cudaMalloc(&S.frame_sgn, ni * sizeof(int))) != cudaSuccess) return E->cuda_fail(e, "frame");
+      if ((e = dmalloc(&S.frame_img, ni * 8)) != cudaSuccess) return E->cuda_fail(e, "frame");
+      if ((e = dmalloc(&S.frame_sgn, ni * sizeof(int))) != cudaSuccess) return E->cuda_fail(e, "frame");
       S.frame_cap = ni;
     }
     cudaMemcpyAsync(S.frame_img, P.frame.rd_img.data(), ni * 8, cudaMemcpyHostToDevice, E->stream);
@@ -1216,6 +1279,35 @@ int finish(pq_engine* E, Slot& S, Plan& P, const std::vector<pq::ExpectPartial>&
   }
   if (in.n_terms_out)
     for (size_t g = 0; g < in.n_gates; ++g) in.n_terms_out[g] = P.gate_op[g] >= 0 ? hist[P.gate_op[g]] : P.n0;
+  S.gate_log.clear();
+  if (P.log) {  // crates/pauli/src/engine.rs:166-193 (GateRecord), one per gate in Heisenberg order
+    std::vector<u64> lg(no * pq::LOG_WORDS);
+    if (no) {
+      cudaMemcpy(lg.data(), S.logs, lg.size() * 8, cudaMemcpyDeviceToHost);
+    }
+    S.gate_log.resize(in.n_gates);
+    for (size_t l = 0; l < in.n_layers; ++l)
+      for (u32 g = in.layer_off[l]; g < in.layer_off[l + 1]; ++g) {
+        pq_gate_record& rcd = S.gate_log[g];
+        rcd = pq_gate_record{};
+        rcd.layer_idx = (u32)l;
+        const long op = P.gate_own[g] ? P.gate_op[g] : -1;
+        rcd.op = (int32_t)op;
+        const u64 after = P.gate_op[g] >= 0 ? hist[P.gate_op[g]] : P.n0;
+        rcd.terms_after = after;
+        rcd.terms_before = op > 0 ? hist[op - 1] : (op == 0 ? P.n0 : after);
+        rcd.terms_gained = rcd.terms_after - std::min(rcd.terms_after, rcd.terms_before);
+        if (op >= 0) {
+          const u64* w = &lg[(size_t)op * pq::LOG_WORDS];
+          rcd.declined = w[pq::LOG_HELD];
+          rcd.emitted = w[pq::LOG_EMITTED];
+          rcd.exchange_hits = w[pq::LOG_HITS];
+          std::memcpy(&rcd.discarded_coeff_l1, &w[pq::LOG_L1], 8);
+          std::memcpy(&rcd.discarded_coeff_max, &w[pq::LOG_MAX], 8);
+          rcd.elapsed_ms = op > 0 ? (double)(stamps[op] - stamps[op - 1]) * 1e-6 : 0.0;
+        }
+      }
+  }
   for (size_t i = 0; i < no; ++i) {
     const u64 n_in = i ? hist[i - 1] : P.n0;
     const double op_ms = i ? (double)(stamps[i] - stamps[i - 1]) * 1e-6 : 0.0;
@@ -1458,6 +1550,7 @@ int run_adjoint(pq_engine* E, const Inputs& in, int W, u32 ckpt_layers, u64 reco
     }
     cudaMemcpyAsync(d_ksrc + b, ksrc.data(), ksrc.size() * sizeof(u64*), cudaMemcpyHostToDevice, E->stream);
     E->h_states[0] = pq::SweepState{};
+    E->init_waits(E->h_states[0]);
     cudaMemcpyAsync(E->d_states, E->h_states, sizeof(pq::SweepState), cudaMemcpyHostToDevice, E->stream);
     pq::AdjointArgs aa{};
     aa.ops = S.d_ops;
@@ -1607,9 +1700,10 @@ int run_batch(pq_engine* E, const std::vector<Inputs>& ins, int WM, const pq_bat
     for (size_t k = 0; k < todo.size(); ++k) {
       Slot& S = E->slots[todo[k]];
       Plan& P = plans[todo[k]];
-      E->h_states[k] = fresh_state(P);
+      E->h_states[k] = fresh_state(E, P);
       cudaMemsetAsync(S.tickets + P.done, 0, (P.ops.size() - P.done) * 4, E->stream);
       E->h_args[k] = sweep_args(S, P, E->d_states + k, off, cnt[k]);
+      E->limit_args(E->h_args[k]);
       E->h_args[k].idle_blocks = rebalance ? E->d_idle : nullptr;
       E->h_args[k].yield_at = yield_at;
       for (u32 b = 0; b < cnt[k]; ++b) E->h_block_inst[off + b] = (u32)k;
@@ -1684,8 +1778,8 @@ int pq_engine_create(pq_engine** out, int device) {
   if (!coop) return PQ_ERR_CUDA;
   E->device = device;
   if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess) return PQ_ERR_CUDA;
-  if (cudaMalloc(&E->d_err, sizeof(u32)) != cudaSuccess) return PQ_ERR_OOM;
-  if (cudaMalloc(&E->d_idle, sizeof(u32)) != cudaSuccess) return PQ_ERR_OOM;
+  if (dmalloc(&E->d_err, sizeof(u32)) != cudaSuccess) return PQ_ERR_OOM;
+  if (dmalloc(&E->d_idle, sizeof(u32)) != cudaSuccess) return PQ_ERR_OOM;
   cudaMemset(E->d_err, 0, sizeof(u32));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1696,7 +1790,19 @@ int pq_engine_create(pq_engine** out, int device) {
   return PQ_OK;
 }
 
-void pq_engine_destroy(pq_engine* E) { delete E; }
+void pq_engine_destroy(pq_engine* E) {
+  BudgetScope scope(E ? &E->budget : nullptr);
+  delete E;
+}
+
+int pq_engine_set_limits(pq_engine* E, const pq_engine_limits* lim) {
+  if (!E) return PQ_ERR_INVALID;
+  E->lim = lim ? *lim : pq_engine_limits{};
+  E->budget.limit = (size_t)E->lim.max_device_bytes;
+  return PQ_OK;
+}
+
+uint64_t pq_engine_device_bytes(const pq_engine* E) { return E ? (uint64_t)E->budget.used : 0; }
 const char* pq_engine_last_error(const pq_engine* E) { return E ? E->err.c_str() : "null engine"; }
 
 }  // extern "C"
@@ -1728,6 +1834,7 @@ extern "C" {
 int pq_run(pq_engine* E, const pq_run_config* cfg, const uint64_t* ow, const double* oc, size_t no,
            const uint64_t* gw, const double* ga, size_t ng, const uint32_t* lo, size_t nl, const uint64_t* d,
            size_t nd, uint64_t* nt, pq_result* r) {
+  BudgetScope scope(E ? &E->budget : nullptr);
   if (!E || !cfg || !r) return PQ_ERR_INVALID;
   std::memset(r, 0, sizeof(*r));
   E->err.clear();
@@ -1742,6 +1849,7 @@ int pq_run(pq_engine* E, const pq_run_config* cfg, const uint64_t* ow, const dou
 }
 
 int pq_run_batch(pq_engine* E, const pq_instance* insts, size_t n, const pq_batch_tuning* tuning) {
+  BudgetScope scope(E ? &E->budget : nullptr);
   if (!E || !insts || !n) return PQ_ERR_INVALID;
   E->err.clear();
   const pq_batch_tuning tune = tuning ? *tuning : pq_batch_tuning{0, 1, 25};
@@ -1774,6 +1882,7 @@ int pq_run_adjoint(pq_engine* E, const pq_run_config* cfg, const uint64_t* ow, c
                    const uint64_t* gw, const double* ga, size_t ng, const uint32_t* lo, size_t nl, const uint64_t* d,
                    size_t nd, uint32_t checkpoint_layers, uint64_t record_bytes, double* grad, uint64_t* nt,
                    pq_result* r) {
+  BudgetScope scope(E ? &E->budget : nullptr);
   if (!E || !cfg || !r || (ng && !grad)) return PQ_ERR_INVALID;
   std::memset(r, 0, sizeof(*r));
   E->err.clear();
@@ -1801,6 +1910,14 @@ size_t pq_result_terms_at(pq_engine* E, size_t index, uint64_t* keys, double* co
 
 size_t pq_result_terms(pq_engine* E, uint64_t* keys, double* coeffs, size_t cap) {
   return pq_result_terms_at(E, 0, keys, coeffs, cap);
+}
+
+size_t pq_result_gates(pq_engine* E, pq_gate_record* out, size_t cap) {
+  if (!E || E->slots.empty()) return 0;
+  const std::vector<pq_gate_record>& g = E->slots[0].gate_log;
+  const size_t m = std::min(g.size(), cap);
+  if (m && out) std::memcpy(out, g.data(), m * sizeof(pq_gate_record));
+  return g.size();
 }
 
 int pq_plugin_load_noise(const char* path, const char* cfg, pq_plugin** out, char* err, size_t n) {

@@ -45,8 +45,6 @@ static_assert(MAX_ITEMS * NWARPS <= 32, "tile scan uses one warp");
 
 constexpr u32 ST_AGG = 1u, ST_INC = 2u;
 constexpr unsigned FULL = 0xffffffffu;
-constexpr long LOOKBACK_SPIN_LIMIT = 1L << 22;  // ~0.3 s with the backoff below
-constexpr long BARRIER_SPIN_LIMIT = 1L << 25;   // ~2 s with the backoff below
 constexpr u32 BAR_GROUPS = SweepState::BAR_GROUPS;
 // A fused op runs both rotations in one pass while each block has at most
 // this many tiles of rows; above, one after the other.
@@ -89,10 +87,11 @@ __device__ __forceinline__ void barrier_release(SweepState* st, u32 g) {
   atomicExch(&st->bar_gen, g + 1);
 }
 __device__ __forceinline__ void barrier_wait(SweepState* st, u32 g) {
-  long spins = 0;
+  const u32 limit = st->barrier_limit;  // set by the host for the launch
+  u32 spins = 0;
   while (*(volatile u32*)&st->bar_gen == g) {
     if (*(volatile u32*)&st->error & ERR_BARRIER_TIMEOUT) break;
-    if (++spins > BARRIER_SPIN_LIMIT) {
+    if (++spins > limit) {
       atomicOr(&st->error, ERR_BARRIER_TIMEOUT);
       break;
     }
@@ -167,7 +166,8 @@ __device__ u32 lookback(u64* status, u32 tile, u32 agg, u32 epoch, SweepState* s
   if (lane == 0) st_volatile(&status[tile], pack_status(epoch, ST_AGG, agg));
   u32 excl = 0;
   long base = (long)tile - 1;
-  long spins = 0;
+  const u32 limit = st->lookback_limit;  // set by the host for the launch
+  u32 spins = 0;
   const u32 ep = epoch & 0x3fffffffu;
   for (;;) {
     const long idx = base - lane;
@@ -184,7 +184,7 @@ __device__ u32 lookback(u64* status, u32 tile, u32 agg, u32 epoch, SweepState* s
     const unsigned inv = __ballot_sync(FULL, flag == 0);
     const unsigned need = inc ? ((inc & (0u - inc)) << 1) - 1 : FULL;  // lanes up to the nearest inclusive
     if (inv & need) {
-      if (++spins > LOOKBACK_SPIN_LIMIT) {
+      if (++spins > limit) {
         if (lane == 0) atomicOr(&st->error, ERR_LOOKBACK_TIMEOUT);
         break;
       }
@@ -477,6 +477,24 @@ __device__ __forceinline__ void record_pair(const SweepArgs& a, const TileSmem& 
   a.rec_idx[o + j] = to_i ? (u32)r : REC_NONE;
 }
 
+// Verbose-log accounting of one source row's sin branch (termsum.rs:604-751):
+// a branch the emit check holds back counts as declined, and as discarded
+// (|b| into the sum and the maximum) unless the partner claims it; a branch
+// that goes out counts as emitted, and as a hit when it lands on an existing
+// row.  |b| >= 0, so its bit pattern orders like the value for atomicMax.
+__device__ __noinline__ void log_branch(u64* log, u32 op, int state, bool sent, bool hit, double b) {
+  u64* l = log + (u64)op * LOG_WORDS;
+  if (state == S_HELD) atomicAdd(l + LOG_HELD, 1ull);
+  if (sent) {
+    atomicAdd(l + LOG_EMITTED, 1ull);
+    if (hit) atomicAdd(l + LOG_HITS, 1ull);
+  } else if (state == S_HELD) {
+    const double m = fabs(b);
+    atomicAdd(reinterpret_cast<double*>(l + LOG_L1), m);
+    atomicMax(l + LOG_MAX, (u64)__double_as_longlong(m));
+  }
+}
+
 // ------------------------------------------------------------------ gate
 // Tiles are assigned statically (tile t to block t mod grid, in order); the
 // cooperative launch keeps every block resident, so a tile's look-back always
@@ -567,6 +585,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
                                   &st->error);
         }
         if (sm.rec_on) record_single(a, sm, r, c[k]);
+        if (a.log) log_branch(a.log, op, si, si == S_EMIT, false, bi);
       } else {
         const double bj = __dmul_rn(__dmul_rn(cj[k], sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
         const int sj = a.host_state ? (int)a.host_state[j[k]] : state(cj[k], key[k]);
@@ -579,6 +598,10 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
         coeffs[r] = ni;
         coeffs[j[k]] = nj;
         if (sm.rec_on) record_pair(a, sm, r, (u64)j[k], c[k], cj[k], to_j, to_i);
+        if (a.log) {
+          log_branch(a.log, op, si, to_j, true, bi);
+          log_branch(a.log, op, sj, to_i, true, bj);
+        }
       }
     }
     unsigned masks[IT];
@@ -666,6 +689,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
           eslot[k] = es;
         }
         if (sm.rec_on) record_single(a, sm, r, c);
+        if (a.log) log_branch(a.log, op, si, si == S_EMIT, false, bi);
       } else {
         const double bj = __dmul_rn(__dmul_rn(cj, sn), neg_im(Ops::template product_exp<W>(g, q), g.sign));
         const int sj = a.host_state ? (int)a.host_state[j] : state(cj, key);
@@ -678,6 +702,10 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
         coeffs[r] = ni;
         coeffs[j] = nj;
         if (sm.rec_on) record_pair(a, sm, r, (u64)j, c, cj, to_j, to_i);
+        if (a.log) {
+          log_branch(a.log, op, si, to_j, true, bi);
+          log_branch(a.log, op, sj, to_i, true, bj);
+        }
       }
     }
     unsigned masks[IT];
@@ -1033,6 +1061,16 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   // live counts, so the offsets agree without communication.
   u64 rb = a.rec_idx ? ld_volatile(&st->rec_next) : 0, rkb = a.rec_idx ? ld_volatile(&st->rec_key_next) : 0;
   bool rec_on = a.rec_idx && !*(volatile u32*)&st->rec_full;
+  if (a.hold_us && grp.bid == a.hold_block && threadIdx.x == 0) {
+    // failure tests only: a bounded hold, so the others' waits on this block expire
+    u64 t0, t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (u32 i = 0; i < (1u << 20); ++i) {  // the host caps hold_us at 100 ms
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      if (t - t0 >= (u64)a.hold_us * 1000ull) break;
+      __nanosleep(1000);
+    }
+  }
   __syncthreads();
   bool stopped = false;  // a capacity stop inside a fused op
   while (op < a.op_end) {

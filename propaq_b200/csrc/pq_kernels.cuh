@@ -51,6 +51,8 @@ struct SweepState {
   u32 grid_stop;  // the sweep stopped at `halt` because the live count outgrew the grid (SweepArgs::grid_rows)
   u32 bar_count;  // grid barrier: groups arrived
   u32 bar_gen;    // grid barrier generation
+  u32 barrier_limit;   // polls a grid-barrier wait makes before it gives up (ERR_BARRIER_TIMEOUT)
+  u32 lookback_limit;  // polls a tile's look-back makes before it gives up (ERR_LOOKBACK_TIMEOUT)
   static constexpr unsigned BAR_GROUPS = 16;
   struct alignas(128) Group {
     u32 count;    // blocks of this group arrived
@@ -108,7 +110,22 @@ struct SweepArgs {
   const unsigned char* host_state;
   const double* host_factor;
   const unsigned char* host_keep;
+  // Per-op emit statistics for the verbose log (null: off), LOG_WORDS words
+  // per op: branches held back by the emit check, the sum and the largest
+  // |branch| of those no partner claimed (double bits), branches that went
+  // out, and those that landed on an existing row.
+  u64* log;
+  // Failure tests (pq_engine_set_limits): block hold_block waits hold_us
+  // microseconds before its first op, so that the other blocks' bounded waits
+  // on it run out.  hold_us 0 = off.
+  u32 hold_block, hold_us;
 };
+
+enum : u32 { LOG_HELD = 0, LOG_L1 = 1, LOG_MAX = 2, LOG_EMITTED = 3, LOG_HITS = 4, LOG_WORDS = 5 };
+
+// Default wait limits (SweepState::barrier_limit / lookback_limit).
+constexpr u32 DEFAULT_BARRIER_POLLS = 1u << 25;   // ~2 s with the back-off of the wait
+constexpr u32 DEFAULT_LOOKBACK_POLLS = 1u << 22;  // ~0.3 s
 
 constexpr u32 REC_NONE = 0xffffffffu;
 

@@ -13,9 +13,15 @@
 // is created when this module is first loaded on a device and is held by that
 // device until the process exits.
 //
-// Set-up: the first call on a device resolves the array's device address
-// with cudaGetSymbolAddress while that device is current.  Make that first
-// call before any stream capture begins.
+// Set-up: every call resolves the array's device address with
+// cudaGetSymbolAddress while the caller's device is current, so the address
+// is right for whatever context is current -- after a cudaDeviceReset (which
+// reloads the module, possibly elsewhere) as well as in a context the caller
+// created itself.  The lookup allocates nothing.  The module (and with it the
+// 16 MiB array) is loaded on a device at the first call there (or when the
+// library is loaded, with CUDA_MODULE_LOADING=EAGER): make that first call
+// before the program reserves its device memory, and before any stream
+// capture begins.
 //
 // Sharing: every call on a device uses the same array, which keeps the last
 // call's contents.  Calls issued concurrently on one device (e.g. from two host
@@ -26,7 +32,6 @@
 
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "../../include/propaq_cuda.h"
@@ -42,12 +47,8 @@ constexpr int NA_MAX_BLOCKS = 512;
 constexpr size_t NA_PARTIALS_BYTES = NA_MAX_BLOCKS * 16;  // (hi, lo) per block
 constexpr size_t NA_RESULT_BYTES = 256;
 constexpr size_t NA_TERMS_OFFSET = NA_PARTIALS_BYTES + NA_RESULT_BYTES;
-constexpr int NA_MAX_DEVICES = 64;
-
 static __device__ __align__(256) unsigned char pq_noalloc_scratch[PQ_NOALLOC_SCRATCH_BYTES];
 
-std::mutex g_mutex;
-void* g_scratch[NA_MAX_DEVICES] = {nullptr};
 thread_local std::string g_error;
 
 __device__ __forceinline__ void na_two_sum(double a, double b, double& s, double& e) {
@@ -165,24 +166,19 @@ int pq_expectation_noalloc_impl(uint32_t basis_kind, uint32_t n_units, const uin
                                        std::to_string((size_t)PQ_NOALLOC_SCRATCH_BYTES) + " bytes");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) {
+  if (e != cudaSuccess) {
     cudaGetLastError();
     return na_fail(PQ_ERR_CUDA, "pq_expectation_noalloc: no current CUDA device");
   }
+  // The array's address in the current context, looked up on every call (see
+  // the set-up note above); a host-side name of the array is not an address
+  // the device can use.
   void* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch[dev]) {  // set-up, once per device, with that device current
-      void* ptr = nullptr;
-      e = cudaGetSymbolAddress(&ptr, pq_noalloc_scratch);
-      if (e != cudaSuccess || !ptr) {
-        cudaGetLastError();
-        return na_fail(PQ_ERR_CUDA, std::string("pq_expectation_noalloc: cudaGetSymbolAddress failed: ") +
-                                        cudaGetErrorString(e));
-      }
-      g_scratch[dev] = ptr;
-    }
-    base = g_scratch[dev];
+  e = cudaGetSymbolAddress(&base, pq_noalloc_scratch);
+  if (e != cudaSuccess || !base) {
+    cudaGetLastError();
+    return na_fail(PQ_ERR_CUDA, std::string("pq_expectation_noalloc: cudaGetSymbolAddress failed: ") +
+                                    cudaGetErrorString(e));
   }
   unsigned char* b = static_cast<unsigned char*>(base);
   double* partials = reinterpret_cast<double*>(b);
@@ -218,7 +214,8 @@ int pq_expectation_noalloc_impl(uint32_t basis_kind, uint32_t n_units, const uin
     case 8: e = na_launch<4, 0>(s, n_units, d_keys, d_coeffs, n_terms, partials, blocks); break;
     case 9: e = na_launch<4, 1>(s, n_units, d_keys, d_coeffs, n_terms, partials, blocks); break;
     case 16: e = na_launch<8, 0>(s, n_units, d_keys, d_coeffs, n_terms, partials, blocks); break;
-    default: e = na_launch<8, 1>(s, n_units, d_keys, d_coeffs, n_terms, partials, blocks); break;
+    case 17: e = na_launch<8, 1>(s, n_units, d_keys, d_coeffs, n_terms, partials, blocks); break;
+    default: return na_fail(PQ_ERR_INVALID, "pq_expectation_noalloc: no kernel for " + std::to_string(W) + " key words");
   }
   if (e != cudaSuccess)
     return na_fail(PQ_ERR_CUDA, std::string("pq_expectation_noalloc: launch failed: ") + cudaGetErrorString(e));

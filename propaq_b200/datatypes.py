@@ -194,6 +194,10 @@ class MajoranaMonomial:
     def commutes_with(self, other: "MajoranaMonomial") -> bool:
         return (self.length * other.length + self.overlap(other)) % 2 == 0
 
+    def resulting_weight(self, other: "MajoranaMonomial") -> int:
+        """Jordan-Wigner weight of the product self @ other (its modes are the XOR)."""
+        return jw_weight(self._modes ^ other._modes, self._n // 2)
+
     def __matmul__(self, other: "MajoranaMonomial"):
         g, k = self._modes, other._modes
         out = g ^ k

@@ -102,6 +102,11 @@ class ZeroCutoffExtrapolator(ABC):
     def build_truncator(self, cutoff):
         """A truncator carrying `cutoff` (None = no cutoff)."""
 
+    def _set_cutoff(self, propagator, cutoff) -> None:
+        """Replaces the matching truncator of the propagator's pipeline
+        (propaq/extrapolators/zce.py:74-88); ValueError if it has none."""
+        propagator.set_truncation(self._pipeline(propagator.truncators, cutoff))
+
     def _pipeline(self, truncators, cutoff):
         truncators = list(truncators)
         idx = next((i for i, t in enumerate(truncators) if isinstance(t, self.truncator_cls())), None)

@@ -35,11 +35,63 @@ class PropagationResult:
 
 
 class Logger:
-    """JSON-lines run log (crates/core/src/interface/logger.rs:19)."""
+    """JSON-lines verbose run log (crates/core/src/interface/logger.rs:13-57).
+
+    A propagator given a Logger rewrites `filename` after each run with the
+    reference's events (crates/pauli/src/propagator.rs:23-101): per gate (every
+    `log_every`-th, Heisenberg order) a `gate` and a `truncation` record, then
+    one `engine_phases` record; propaq's LogParser reads it.  The engine runs
+    such a run with every rotation as an op of its own, so ms_per_gate is that
+    op's device time.  The engine has no scan / absorb / claims phases: its
+    gate ops do all three, and their device time is reported as scan_s.
+    """
 
     def __init__(self, filename: str, log_every: int = 1):
         self.filename = filename
         self.log_every = max(1, int(log_every))
+
+
+def _rust_exp(x: float, digits: int) -> str:
+    """Rust's `{:.Ne}` formatting of a float (e.g. 1.234e-2, 0.000e0)."""
+    m, e = f"{x:.{digits}e}".split("e")
+    return f"{m}e{int(e)}"
+
+
+def write_gate_log(logger: Logger, records, qiskit_idx, cfg, res) -> None:
+    """The reference's write_gate_log (crates/pauli/src/propagator.rs:23-101)
+    from the engine's per-gate records."""
+    every = logger.log_every
+    wc = "null" if cfg.weight is None else str(int(cfg.weight))
+    cc = _rust_exp(0.0 if cfg.coefficient is None else float(cfg.coefficient), 6)
+    lines = []
+    tot_decl = tot_emit = tot_hits = 0
+    for g, r in enumerate(records):
+        tot_decl += r.declined
+        tot_emit += r.emitted
+        tot_hits += r.exchange_hits
+        if g % every:
+            continue
+        q = qiskit_idx[g]
+        qk = "null" if q is None else str(int(q))
+        lines.append(f'{{"event":"gate","gate_idx":{g},"layer_idx":{r.layer_idx},"qiskit_gate_idx":{qk},'
+                     f'"terms":{r.terms_after},"ms_per_gate":{_rust_exp(r.elapsed_ms, 3)}}}')
+        lines.append(f'{{"event":"truncation","gate_idx":{g},"layer_idx":{r.layer_idx},"qiskit_gate_idx":{qk},'
+                     f'"trigger":"emit","truncation_model":"emit_gate","terms_before":{r.terms_before},'
+                     f'"terms_after":{r.terms_after},"terms_gained":{r.terms_gained},"terms_discarded":{r.declined},'
+                     f'"discarded_coeff_l1":{_rust_exp(r.discarded_coeff_l1, 6)},'
+                     f'"discarded_coeff_max":{_rust_exp(r.discarded_coeff_max, 6)},"weight_cutoff":{wc},'
+                     f'"coeff_cutoff":{cc},"elapsed_ms":{_rust_exp(r.elapsed_ms, 3)}}}')
+    visited = int(res.sum_anti)
+    share = lambda part, whole: part / max(whole, 1)  # noqa: E731
+    lines.append(json.dumps({
+        "event": "engine_phases", "partitions": 1, "scan_s": res.gate_ms * 1e-3, "absorb_s": 0.0, "claims_s": 0.0,
+        "scan_occupancy": 1.0, "absorb_occupancy": 0.0, "claims_occupancy": 0.0, "terms": int(res.n_final),
+        "inline_positions": 0, "overflow_rows": 0, "overflow_share": 0.0, "visited": visited,
+        "emitted": int(tot_emit), "declined": int(tot_decl), "emitted_share": share(tot_emit, visited),
+        "declined_share": share(tot_decl, visited), "exchange_hits": int(tot_hits),
+        "exchange_hit_share": share(tot_hits, tot_emit)}, separators=(",", ":")))
+    with open(logger.filename, "w") as f:
+        f.write("\n".join(lines) + "\n")
 
 
 def heisenberg_gates(circuit, n_words: int, key_of):
@@ -147,6 +199,7 @@ class _Propagator:
         if plugin is not None:
             rc.noise_plugin = plugin.handle
         rc.want_terms = 1 if want_terms else 0
+        rc.log_gates = 1 if self.logger is not None else 0
         obs_keys, obs_coeffs = observable.to_arrays(n_words)
         gw, ga, off = heisenberg_gates(circuit, n_words, self._key)
         diag = None if initial_state is None else state_words(initial_state, n_units)
@@ -168,17 +221,10 @@ class _Propagator:
         self.last_run = res
         terms = eng.terms(n_words) if want_terms else None
         if self.logger is not None:
-            self._write_log(res, nt, n_units)
+            rots = [r for layer in reversed(list(circuit.layers)) for r in list(layer)[::-1]]
+            write_gate_log(self.logger, eng.gates(), [getattr(r, "qiskit_gate_idx", None) for r in rots],
+                           keep[2], res)
         return res, nt, terms, n_words
-
-    def _write_log(self, res, nt, n_units):
-        with open(self.logger.filename, "a") as f:
-            for g, n in enumerate(nt):
-                if g % self.logger.log_every == 0:
-                    f.write(json.dumps({"event": "gate", "gate_idx": g, "terms_after": int(n)}) + "\n")
-            f.write(json.dumps({"event": "engine_phases", "terms": int(res.n_final), "peak_terms": int(res.peak_terms),
-                                "device_ms": res.device_ms, "gpu_launches": int(res.gpu_launches),
-                                "n_units": n_units}) + "\n")
 
     def propagate(self, observable, circuit, filename=None):
         """Back-propagates `observable` through `circuit`; returns the evolved term sum."""

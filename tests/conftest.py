@@ -6,6 +6,9 @@ from pathlib import Path
 import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
+# The reference's source tree, read only by CPU tests that load its pure-Python
+# modules or stub files; they skip when it is absent (as on a GPU box).
+REFERENCE_TREE = Path(os.environ.get("PROPAQ_REFERENCE", "/root/reference"))
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(Path(__file__).resolve().parent))
 

@@ -8,7 +8,8 @@ noise / truncation.  This script rebuilds that circuit exactly as the notebook
 does and reads the printed values out of the stored notebook outputs, so the
 fixture carries both the inputs and the reference's own answers.
 
-Run from the repository root:  python tests/golden/make_golden.py [/root/reference]
+Run from the repository root:  python tests/golden/make_golden.py <reference tree>
+(or with the tree in the PROPAQ_REFERENCE environment variable).
 """
 
 import json
@@ -17,7 +18,11 @@ import re
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+import os
+
+if len(sys.argv) < 2 and not os.environ.get("PROPAQ_REFERENCE"):
+    sys.exit("usage: make_golden.py <reference tree>  (or set PROPAQ_REFERENCE)")
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ["PROPAQ_REFERENCE"])
 NB = REF / "examples" / "plugins" / "notebooks"
 OUT = Path(__file__).resolve().parent / "plugin_notebooks.json"
 N_QUBITS = 4

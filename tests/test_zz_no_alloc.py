@@ -68,3 +68,37 @@ def test_noalloc_expectation_majorana_and_refusal(gpu_engine, oracle):
     n = SCRATCH_BYTES // 16
     rc, _, msg = noalloc(0, 20, np.zeros((n, 1), np.uint64), np.zeros(n), np.zeros(1, np.uint64))
     assert rc == _native.PQ_ERR_INVALID and "static scratch" in msg
+
+
+@pytest.mark.parametrize("n_units,basis", [(50, 0), (100, 0), (200, 0), (48, 1), (100, 1)])
+def test_noalloc_every_key_width(gpu_engine, oracle, n_units, basis):
+    """2-, 4- and 8-word keys (Pauli 50 / 100 / 200 qubits, Majorana 48 / 100
+    sites) against pq_run's expectation of the same final terms and the
+    oracle's, on two calls in a row."""
+    from harness import from_workload, random_pauli_problem, spread_units
+
+    from propaq_b200 import workloads
+
+    if basis == 0:
+        # a dozen active qubits spread over the register, so keys use every word
+        p = random_pauli_problem(40 + n_units, n_units, n_gates=70, layer_size=6, max_weight=5, min_coeff=1e-5,
+                                 units=spread_units(n_units, n_units, 12))
+    else:
+        p = from_workload(workloads.majorana_givens(n_sites=n_units, reps=1, max_weight=5, min_coeff=1e-5))
+    assert p.n_words == {50: 2, 100: 4, 200: 8, 48: 2}[n_units]
+    g = run_gpu(gpu_engine, p)
+    o = run_oracle(oracle, p)
+    assert len(g.coeffs) > 1
+    for _ in range(2):
+        rc, value, msg = noalloc(p.basis, p.n_units, g.keys, g.coeffs, p.diag)
+        assert rc == 0, msg
+        assert expectation_close(value, o)[0], (value, o.expectation_accurate)
+        assert abs(value - g.expectation) <= 1e-12 * abs(g.expectation) + 4 * np.finfo(float).eps * o.expectation_abs
+
+
+def test_noalloc_zero_terms_and_unit_limit(gpu_engine):
+    """No terms give 0.0; more than 256 units are refused before any device work."""
+    rc, value, msg = noalloc(0, 20, np.zeros((0, 1), np.uint64), np.zeros(0), np.zeros(1, np.uint64))
+    assert rc == 0 and value == 0.0, msg
+    rc, _, msg = noalloc(1, 257, np.zeros((1, 16), np.uint64), np.ones(1), np.zeros(5, np.uint64))
+    assert rc == _native.PQ_ERR_INVALID and "256-unit" in msg
