@@ -113,6 +113,8 @@ typedef struct pq_result {
   uint64_t sum_rows_phase;    /* sum over phase-only ops of the rows they scan */
   uint64_t sum_rows_noise;    /* sum over noise ops of the rows they scan      */
   uint64_t sum_kept;          /* ... of the rows a reclaim keeps               */
+  uint64_t class_ops;         /* ops that ran a class of rotations (generators on
+                                 disjoint units) through one pass              */
 } pq_result;
 
 /* Key width for a register: 1,2,4,...,64 words for up to 32,64,...,2048
@@ -196,9 +198,11 @@ typedef struct pq_gate_record {
   int32_t op;                         /* the gate's op in the sweep; -1 = deferred */
 } pq_gate_record;
 
-/* Per-gate records of the last pq_run made with log_gates, gates in
- * Heisenberg order.  Writes min(cap, n) records, returns n (0 without
- * log_gates). */
+/* Per-gate records of the last pq_run, gates in Heisenberg order: live
+ * counts and device time after every run (a fused op's time goes to its first
+ * rotation), the emit statistics (declined, emitted, exchange_hits, the
+ * discarded mass) only after a run made with log_gates.  Writes min(cap, n)
+ * records, returns n. */
 size_t pq_result_gates(pq_engine* engine, pq_gate_record* out, size_t cap);
 
 /* One propagation of a batch: the arguments of pq_run in one record.  Keys

@@ -97,6 +97,7 @@ class RunResult(ctypes.Structure):
         ("sum_rows_phase", ctypes.c_uint64),
         ("sum_rows_noise", ctypes.c_uint64),
         ("sum_kept", ctypes.c_uint64),
+        ("class_ops", ctypes.c_uint64),
     ]
 
 

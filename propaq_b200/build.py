@@ -24,7 +24,7 @@ LIB = LIB_DIR / "libpropaq_cuda.so"
 # include pq_kernels.cu) so that they compile in parallel with the rest.
 SOURCES = ["pq_kernels_w64.cu", "pq_kernels_w32.cu", "pq_kernels_w16.cu", "pq_kernels.cu", "pq_host.cu",
            "pq_noalloc.cu"]
-HEADERS = ["pq_device.cuh", "pq_kernels.cuh", "pq_tableau.h"]
+HEADERS = ["pq_device.cuh", "pq_kernels.cuh", "pq_tableau.h", "pq_class.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -50,27 +50,51 @@ def _stale() -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
+OBJ_DIR = PKG / "_build"  # objects, kept for incremental builds (not shipped with the library)
+
+
+def _obj(src: str) -> Path:
+    return OBJ_DIR / (Path(src).stem + ".o")
+
+
+def _obj_stale(src: str) -> bool:
+    """An object is rebuilt when it is missing or older than its source, a
+    shared header or the C ABI header (every source includes them)."""
+    obj = _obj(src)
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    deps = [CSRC / src] + [CSRC / h for h in HEADERS] + [PKG.parent / "include" / "propaq_cuda.h"]
+    if src.startswith("pq_kernels_w"):  # the wide-key units include pq_kernels.cu
+        deps.append(CSRC / "pq_kernels.cu")
+    return any(d.stat().st_mtime > t for d in deps)
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compiles the engine if any source is newer than the library."""
+    """Compiles the engine if any source is newer than the library; only the
+    translation units whose inputs changed are recompiled (objects are kept
+    beside the library)."""
     if not force and not _stale():
         return LIB
     LIB_DIR.mkdir(exist_ok=True)
+    OBJ_DIR.mkdir(exist_ok=True)
 
     def compile_one(src):
-        obj = LIB_DIR / (Path(src).stem + ".o")
+        obj = _obj(src)
         cmd = [nvcc(), *NVCC_FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
         return src, str(obj), subprocess.run(cmd, capture_output=True, text=True)
 
-    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as pool:
-        results = list(pool.map(compile_one, SOURCES))
-    objs = []
+    todo = [s for s in SOURCES if force or _obj_stale(s)]
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo) or 1, os.cpu_count() or 1))) as pool:
+        results = list(pool.map(compile_one, todo))
     for src, obj, r in results:
         if r.returncode != 0:
+            Path(obj).unlink(missing_ok=True)
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError(f"nvcc failed on {src}")
         if verbose:
             sys.stderr.write(r.stderr)
-        objs.append(obj)
+    objs = [str(_obj(s)) for s in SOURCES]
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", str(tmp), "-ldl"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -78,8 +102,6 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("nvcc link failed")
     os.replace(tmp, LIB)
-    for o in objs:
-        Path(o).unlink(missing_ok=True)
     return LIB
 
 

@@ -27,6 +27,7 @@ enum : u32 {
   ERR_PROBE_OVERFLOW = 2u,    // a hash probe ran past the table size
   ERR_CAPACITY = 4u,          // a write would have passed the row capacity
   ERR_BARRIER_TIMEOUT = 8u,   // a grid barrier wait expired
+  ERR_CLASS_FAMILY = 16u,     // a row's family in a class op exceeded CLASS_KMAX (the host rules it out)
 };
 
 __host__ __device__ inline int mod4(int v) { return v & 3; }

@@ -1029,6 +1029,8 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
   }
 }
 
+#include "pq_class.cuh"
+
 // Runs ops [a.op_begin, a.op_end) of one propagation on the blocks of `grp`.
 template <int W, int ALG>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
@@ -1049,7 +1051,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     const OpDesc d = a.ops[k];
     sod = d;
     const GateDesc<W>* gd = reinterpret_cast<const GateDesc<W>*>(a.gates);
-    if (d.kind != OP_NOISE_SCALE && d.kind != OP_NOISE_COMPACT)
+    if (d.kind != OP_NOISE_SCALE && d.kind != OP_NOISE_COMPACT && !is_class(d.kind))
       for (u32 i = 0; i < fused_count(d.kind); ++i) sgs[i] = gd[d.idx + i];
   };
   if (threadIdx.x == 0) {
@@ -1124,6 +1126,18 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
         if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, N);
       } else if (N == 0) {
         if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
+      } else if (is_class(od.kind)) {
+        const GateDesc<W>* gd = reinterpret_cast<const GateDesc<W>*>(a.gates) + od.idx;
+        int rc = 1;
+        if constexpr (W <= 4)
+          rc = class_op<W, ALG>(a, gd, nops, op, N, keys, coeffs, sm, grp, n_out, gen);
+        else if (threadIdx.x == 0)  // the host forms classes for keys of at most 4 words
+          atomicOr(&st->error, ERR_CLASS_FAMILY);
+        if (rc == 2) {  // capacity: stopped before any write, st->halt is set
+          stopped = true;
+          break;
+        }
+        // rc 1: a device error; the barrier below ends the sweep
       } else if (nops == 2 && N <= (u64)grp.nblk * BLOCK * GATE2_TILES_PER_BLOCK && 4 * N <= a.cap) {
         gate2_tiles<W, ALG>(a, sgs[0], sgs[1], op, N, keys, coeffs, sm, grp, n_out);
       } else {  // many rows: the rotations one after the other (op + i is rotation i's slot)
@@ -1168,7 +1182,8 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     // the same branch (a block reading late sees a later op and goes on).
     if (a.idle_blocks && grp.bid == 0 && threadIdx.x == 0 && *(volatile u32*)a.idle_blocks >= a.yield_at)
       *(volatile u32*)&st->yield_after = op + 1;
-    op_barrier(st, gen, grp, n_out, nops > 1 && !split ? a.tickets + op : nullptr, nops - 1, os,
+    const bool cls = is_class(od.kind) && !split;
+    op_barrier(st, gen, grp, n_out, nops > 1 && !split && !cls ? a.tickets + op : nullptr, nops - 1, os,
                [&] { fetch_op(op + nops); });
     par ^= 1u;
     if (os.err) {
@@ -1178,7 +1193,13 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     if (grp.bid == 0 && threadIdx.x == 0) {
       const u64 n_new = os.n;
       a.hist[op + nops - 1] = n_new;
-      if (nops > 1 && !split) {  // counts after each rotation of the group but the last
+      if (cls) {  // counts after each rotation of the class: the rows each one created
+        u64 acc = N;
+        for (u32 i = 0; i + 1 < nops; ++i) {
+          acc += *(volatile u32*)(a.tickets + op + i);
+          a.hist[op + i] = acc;
+        }
+      } else if (nops > 1 && !split) {  // counts after each rotation of the group but the last
         u64 acc = N;
         for (u32 i = 0; i + 1 < nops; ++i) {
           acc += os.extra[i];

@@ -17,12 +17,23 @@ enum OpKind : u32 {
   OP_GATE_TAIL = 5,      // a later rotation of such a group: run by its head, skipped by the sweep
   OP_GATE3 = 6,
   OP_GATE4 = 7,
+  // A class: the next m rotations (m in the bits above the low byte), whose
+  // generators act on pairwise disjoint units, in one op (class_op).
+  OP_CLASS = 8,
 };
 
-// Rotations run by an op: 2 to 4 for a fused group's head, else 1.
+// A class op's kind word: OP_CLASS with its rotation count above the low byte.
+__host__ __device__ inline u32 class_kind(u32 m) { return OP_CLASS | (m << 8); }
+__host__ __device__ inline bool is_class(u32 kind) { return (kind & 0xffu) == OP_CLASS; }
+
+// Rotations run by an op: 2 to 4 for a fused group's head, m for a class, else 1.
 __host__ __device__ inline u32 fused_count(u32 kind) {
+  if (is_class(kind)) return kind >> 8;
   return kind == OP_GATE2 ? 2u : (kind == OP_GATE3 ? 3u : (kind == OP_GATE4 ? 4u : 1u));
 }
+
+constexpr u32 CLASS_MAX = 64;   // rotations of one class op (a row's class mask is one u64)
+constexpr u32 CLASS_KMAX = 10;  // largest family dimension (class rotations one row anticommutes with)
 
 struct OpDesc {
   u32 kind;
@@ -33,6 +44,9 @@ template <int W>
 struct GateDesc {
   GenInfo<W> g;
   double sn, cs;  // sin(angle), cos(angle) from the host libm
+  u32 pivot;      // in a class: a key bit of this generator that no other
+                  // generator of the class has (its family coordinate)
+  u32 pad_;
 };
 
 // Device-resident state of a sweep, one per engine.
@@ -51,6 +65,7 @@ struct SweepState {
   u32 grid_stop;  // the sweep stopped at `halt` because the live count outgrew the grid (SweepArgs::grid_rows)
   u32 bar_count;  // grid barrier: groups arrived
   u32 bar_gen;    // grid barrier generation
+  u64 need_rows;       // rows a class op stopped for (its output), for the host's growth
   u32 barrier_limit;   // polls a grid-barrier wait makes before it gives up (ERR_BARRIER_TIMEOUT)
   u32 lookback_limit;  // polls a tile's look-back makes before it gives up (ERR_LOOKBACK_TIMEOUT)
   static constexpr unsigned BAR_GROUPS = 16;
@@ -110,6 +125,15 @@ struct SweepArgs {
   const unsigned char* host_state;
   const double* host_factor;
   const unsigned char* host_keep;
+  // Class ops (null without them): per row, the mask of class rotations it
+  // anticommutes with and the slot of its family; per family owner, the rows
+  // the family creates; the family table (slots (fingerprint << 32) | first
+  // row, table_mask + 1 of them) and per slot (count << 32) | (~ least row).
+  u64* cls_mask;
+  u32* cls_slot;
+  u32* cls_children;
+  u64* fam_table;
+  u64* fam_aux;
   // Per-op emit statistics for the verbose log (null: off), LOG_WORDS words
   // per op: branches held back by the emit check, the sum and the largest
   // |branch| of those no partner claimed (double bits), branches that went
