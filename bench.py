@@ -68,7 +68,10 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true",
                     help="batch: time the given --blocks-per-sm/--split/--rebalance-pct instead of the autotuner's")
     ap.add_argument("--checkpoint-layers", type=int, default=3, help="adjoint: layers per checkpoint segment")
-    ap.add_argument("--shift-sample", type=int, default=96, help="adjoint: parameter-shift evaluations timed")
+    ap.add_argument("--shift-sample", type=int, default=480,
+                    help="adjoint: parameter-shift evaluations timed in batches of 8")
+    ap.add_argument("--shift-sequential", type=int, default=96,
+                    help="adjoint: parameter-shift evaluations timed as plain pq_run calls")
     return ap.parse_args()
 
 
@@ -479,6 +482,8 @@ def main_adjoint(args, world, rank, local):
     dev_ms = fwd_ms = 0.0
     launches = 0
     e2e_s = 0.0
+    alg = 0.0
+    W = _native.words_for_units(wl.n_units)
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             settle()
@@ -486,8 +491,18 @@ def main_adjoint(args, world, rank, local):
             fwd_ms += prop.last_run.device_ms
             settle()
             e, g = spec.value_and_grad(th)
-            dev_ms += prop.last_run.device_ms
-            launches += int(prop.last_run.gpu_launches)
+            r = prop.last_run
+            dev_ms += r.device_ms
+            launches += int(r.gpu_launches)
+            # algorithmic bytes: the forward sweep (as the plain bench) and the
+            # reverse sweep: per gate op keys, lambda in and out of every row,
+            # the record (coefficient + partner index) and the partner's lambda
+            # of every anticommuting row; per noise op keys, both lambdas and
+            # the reclaim map
+            fwd = (gate_bytes(W, r.sum_rows_gate, r.sum_anti, r.sum_children) + 8 * W * r.sum_rows_phase
+                   + (8 * W + 16) * (r.sum_rows_noise + r.sum_kept))
+            rev = (8 * W + 16) * (r.sum_rows_gate + r.sum_rows_phase) + 20 * r.sum_anti + (8 * W + 20) * r.sum_rows_noise
+            alg += fwd + rev
         for _ in range(args.steps):
             settle()
             t0 = time.perf_counter()
@@ -495,26 +510,38 @@ def main_adjoint(args, world, rank, local):
             spec(th_req).backward()
             _ = th_req.grad.numpy().sum()
             e2e_s += time.perf_counter() - t0
-        # Parameter shift: a timed sample of its 2 x 1200 propagations, 8 at a
-        # time through pq_run_batch, scaled to the full count.
+        # Parameter shift: timed samples of its 2 x 1200 propagations, spread
+        # over the angles, scaled to the full count: one plain pq_run call per
+        # evaluation, and 8 evaluations per pq_run_batch call.
         base = spec._call_args(th)
         eng = _native.engine(local)
         items = []
-        for k in range(args.shift_sample):
+        step = max(1, n_shift // args.shift_sample)
+        for k in range(0, n_shift, step):
             gi = spec._param_gates[(k // 2) % len(spec._param_gates)]
             a = base[4].copy()
             a[gi] += (1 if k % 2 == 0 else -1) * math.pi / 2
             items.append(tuple(base[:4]) + (a,) + tuple(base[5:]))
+        items = items[:args.shift_sample]
         settle()
         ps_ms = 0.0
         for i in range(0, len(items), 8):
             out = eng.run_batch(items[i:i + 8], want_n_terms=False)
             ps_ms += out[0][0].device_ms
+        settle()
+        seq_ms = 0.0
+        n_seq = min(len(items), args.shift_sequential)
+        for it in items[:n_seq]:
+            res, _ = eng.run(*it, want_n_terms=False)
+            seq_ms += res.device_ms
     clocks = clk.summary()
     dev_s = max_over_ranks(world, dev_ms / 1e3)
     e2e_s = max_over_ranks(world, e2e_s)
     shift_ms = ps_ms / len(items) * n_shift
+    seq_shift_ms = seq_ms / max(1, n_seq) * n_shift
     h2d = sum(int(np.asarray(x).nbytes) for x in base[1:] if x is not None) + 8 * len(th)
+    peak_gbs, peak_kind = measured_peaks()
+    achieved = alg / (dev_ms / 1e3) / 1e9 if dev_ms > 0 else None
     line = dict(base_line, value=world * args.steps / dev_s, ms_per_step=1e3 * dev_s / args.steps,
                 forward_ms=fwd_ms / args.steps, expectation_value=e,
                 e2e={"value": world * args.steps / e2e_s, "unit": "gradients/s", "h2d_bytes_per_step": int(h2d),
@@ -522,10 +549,37 @@ def main_adjoint(args, world, rank, local):
                      "path": "torch.autograd: ParametrizedExpectation(theta).backward()"},
                 gpu_launches=launches // max(1, args.steps),
                 parameter_shift={"evaluations": n_shift, "timed_sample": len(items),
+                                 "sample": f"every {step}th of the {n_shift} shifted circuits",
                                  "ms_per_evaluation": ps_ms / len(items), "ms_per_gradient": shift_ms,
                                  "how": "pq_run_batch, 8 shifted circuits per call, device time",
-                                 "adjoint_speedup": shift_ms / (1e3 * dev_s / args.steps)},
-                roofline=None, clocks=clocks)
+                                 "adjoint_speedup": shift_ms / (1e3 * dev_s / args.steps),
+                                 "sequential": {"timed_sample": n_seq, "ms_per_evaluation": seq_ms / max(1, n_seq),
+                                                "ms_per_gradient": seq_shift_ms,
+                                                "how": "one pq_run call per shifted circuit, device time",
+                                                "adjoint_speedup": seq_shift_ms / (1e3 * dev_s / args.steps)}},
+                roofline={"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+                          "frac": None if achieved is None else achieved / peak_gbs, "traffic": None,
+                          "kernel": "sweep_kernel + adjoint_kernel", "peak_source": f"{peak_kind} hbm_gbs",
+                          "algorithmic_bytes_per_gradient": alg / args.steps,
+                          "note": "forward sweep and reverse sweep bytes over the gradient's device time"},
+                clocks=clocks)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference has no gradient: its CPU path is parameter shift on the
+        # oracle, timed on a bounded sample of evaluations
+        o = oracle_load()
+        p = from_workload(wl)
+        n_eval, t0 = 0, time.perf_counter()
+        while n_eval < 2 or time.perf_counter() - t0 < args.cpu_seconds:
+            gi = spec_cpu._param_gates[(n_eval // 2) % len(spec_cpu._param_gates)]
+            p.angles = base[4].copy()
+            p.angles[gi] += (1 if n_eval % 2 == 0 else -1) * math.pi / 2
+            run_oracle(o, p, n_partitions=cores, want_terms=False)
+            n_eval += 1
+        el = time.perf_counter() - t0
+        v = 1.0 / (el / n_eval * n_shift)
+        line["cpu_baseline"] = {"value": v, "unit": "gradients/s", "cores": cores, "kind": "port",
+                                "sample": f"{n_eval} parameter-shift evaluations in {el:.1f} s on the oracle "
+                                          f"({cores} threads), scaled to {n_shift}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -80,7 +80,9 @@ typedef struct pq_run_config {
   const double* noise_tables;/* TABLE / LAYERED factors                         */
   size_t noise_table_len;    /* entries per table (normally n_units + 1)       */
   const pq_plugin* noise_plugin; /* PLUGIN kind                                 */
-  uint32_t want_terms;       /* keep the final terms for pq_result_terms        */
+  uint32_t want_terms;       /* keep the final terms for pq_result_terms: 1 in
+                                the engine's row order, 2 sorted by key (as a
+                                64 n_words-bit integer, on the device)          */
   uint32_t blocks_per_sm;    /* sweep blocks per SM; 0 = by live count: 1 while
                                 every row has a thread, 2 up to 2^20 rows, then
                                 as many as fit (a launch stops and is relaunched

@@ -23,8 +23,8 @@ LIB = LIB_DIR / "libpropaq_cuda.so"
 # The 16-, 32- and 64-word kernels are separate translation units (they
 # include pq_kernels.cu) so that they compile in parallel with the rest.
 SOURCES = ["pq_kernels_w64.cu", "pq_kernels_w32.cu", "pq_kernels_w16.cu", "pq_kernels.cu", "pq_host.cu",
-           "pq_noalloc.cu"]
-HEADERS = ["pq_device.cuh", "pq_kernels.cuh", "pq_tableau.h", "pq_class.cuh"]
+           "pq_noalloc.cu", "pq_sort.cu"]
+HEADERS = ["pq_device.cuh", "pq_kernels.cuh", "pq_tableau.h", "pq_class.cuh", "pq_sort.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -57,16 +57,27 @@ def _obj(src: str) -> Path:
     return OBJ_DIR / (Path(src).stem + ".o")
 
 
+# What each translation unit includes (besides itself).
+_KERNEL_DEPS = ["pq_device.cuh", "pq_kernels.cuh", "pq_class.cuh"]
+DEPS = {
+    "pq_kernels.cu": _KERNEL_DEPS,
+    "pq_kernels_w16.cu": _KERNEL_DEPS + ["pq_kernels.cu"],
+    "pq_kernels_w32.cu": _KERNEL_DEPS + ["pq_kernels.cu"],
+    "pq_kernels_w64.cu": _KERNEL_DEPS + ["pq_kernels.cu"],
+    "pq_host.cu": ["pq_device.cuh", "pq_kernels.cuh", "pq_sort.cuh", "pq_tableau.h", "../../include/propaq_cuda.h"],
+    "pq_noalloc.cu": ["pq_device.cuh", "../../include/propaq_cuda.h"],
+    "pq_sort.cu": ["pq_device.cuh", "pq_sort.cuh"],
+}
+
+
 def _obj_stale(src: str) -> bool:
-    """An object is rebuilt when it is missing or older than its source, a
-    shared header or the C ABI header (every source includes them)."""
+    """An object is rebuilt when it is missing or older than its source or a
+    file it includes."""
     obj = _obj(src)
     if not obj.exists():
         return True
     t = obj.stat().st_mtime
-    deps = [CSRC / src] + [CSRC / h for h in HEADERS] + [PKG.parent / "include" / "propaq_cuda.h"]
-    if src.startswith("pq_kernels_w"):  # the wide-key units include pq_kernels.cu
-        deps.append(CSRC / "pq_kernels.cu")
+    deps = [CSRC / src] + [CSRC / h for h in DEPS[src]]
     return any(d.stat().st_mtime > t for d in deps)
 
 

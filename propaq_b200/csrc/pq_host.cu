@@ -33,6 +33,7 @@
 
 #include "../../include/propaq_cuda.h"
 #include "pq_kernels.cuh"
+#include "pq_sort.cuh"
 #include "pq_tableau.h"
 
 using pq::u32;
@@ -51,6 +52,10 @@ constexpr double EPS_CLASSIFY = 1e-9;  // termsum.rs:42, partitioned_termsum.rs:
 constexpr u32 MAX_UNITS = 2048;        // engine.rs:27
 constexpr u64 MAX_ROWS = 1ULL << 31;   // row index ceiling of the table slots
 constexpr int TILE_ROWS = 256;  // smallest tile a sweep uses (sizes the look-back status array)
+// Observables of at least this many admitted terms fold their duplicate keys
+// on the device (radix sort by key, then a sum over each run of equal keys);
+// smaller ones on the host.
+constexpr size_t DEVICE_FOLD_MIN = 1u << 15;
 
 // --------------------------------------------------------------- plugins
 struct Plugin {
@@ -361,6 +366,7 @@ struct pq_engine {
   // and per-op arrays, the segment checkpoints, and the pool size the last
   // default-sized gradient needed to record every op.
   DevBuf g_pool, g_lam, g_ops;
+  DevBuf sort_buf;  // radix-sort scratch and sorted rows (observable folding, sorted term output)
   std::vector<DevBuf> g_ck;
   size_t g_need = 0;
   // pq_engine_set_limits: the row ceiling, the device-memory budget the
@@ -400,7 +406,7 @@ struct pq_engine {
   ~pq_engine() {
     if (stream) cudaStreamSynchronize(stream);
     for (auto& s : slots) s.free_all();
-    for (DevBuf* b : {&g_pool, &g_lam, &g_ops}) b->release();
+    for (DevBuf* b : {&g_pool, &g_lam, &g_ops, &sort_buf}) b->release();
     for (DevBuf& b : g_ck) b.release();
     for (void* p : {(void*)d_states, (void*)d_args, (void*)d_block_inst, (void*)d_err, (void*)d_idle})
       if (p) dfree(p);
@@ -574,6 +580,7 @@ struct Plan {
   bool defer = true;
   bool log = false;  // per-gate records for the verbose log (pq_run_config::log_gates)
   bool has_class = false;  // some op is a class (fuse_classes)
+  bool fold_on_device = false;  // hk / hc hold the admitted terms unfolded (DEVICE_FOLD_MIN)
   std::vector<u64> hk;
   std::vector<double> hc;
   u64 n0 = 0;
@@ -665,6 +672,7 @@ int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
   };
   std::unordered_map<std::vector<u64>, size_t, H> pos;
   std::vector<u64> k(W);
+  P.fold_on_device = in.n_obs >= DEVICE_FOLD_MIN;
   for (size_t i = 0; i < in.n_obs; ++i) {
     P.widen(in.obs_words, i, k.data());
     const double c = in.obs_coeffs[i];
@@ -676,6 +684,11 @@ int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
     } else {
       if (P.has_w && host_weight(ALG, W, k.data(), P.n_units) > P.wcut) continue;
       if (P.has_c && !(std::fabs(c) >= P.ccut)) continue;
+    }
+    if (P.fold_on_device) {  // folded by setup_slot on the device, in this order
+      P.hk.insert(P.hk.end(), k.begin(), k.end());
+      P.hc.push_back(c);
+      continue;
     }
     auto it = pos.find(k);
     if (it != pos.end()) {
@@ -706,7 +719,29 @@ int setup_slot(pq_engine* E, Slot& S, Plan& P) {
     if (int rc = E->resize(S, std::max(want_cap, S.W == W ? S.cap : 0), 0, S.cur, W)) return rc;
   }
   S.cur = 0;
-  if (P.n0) {
+  if (P.n0 && P.fold_on_device) {
+    // duplicates add up as the host loop would: stable sort by key, then each
+    // run of equal keys summed in input order (engine.rs:104-111)
+    cudaMemcpyAsync(S.keys[1], P.hk.data(), P.n0 * W * 8, cudaMemcpyHostToDevice, E->stream);
+    cudaMemcpyAsync(S.coeffs[1], P.hc.data(), P.n0 * 8, cudaMemcpyHostToDevice, E->stream);
+    const u64 words = pq::sort_scratch_words(P.n0, W) + (P.n0 + 1) / 2;
+    if ((e = E->sort_buf.ensure(words * 8)) != cudaSuccess) return E->cuda_fail(e, "sort scratch");
+    u64* scratch = E->sort_buf.at<u64>(0);
+    u32* head = reinterpret_cast<u32*>(scratch + pq::sort_scratch_words(P.n0, W));
+    u64 n_fold = 0;
+    e = with_words(W, [&](auto w) {
+      constexpr int WW = decltype(w)::value;
+      cudaError_t ee = pq::sort_rows<WW>(S.keys[1], S.coeffs[1], P.n0, S.keys[0], S.coeffs[0], scratch, E->stream,
+                                         &E->launches);
+      if (ee == cudaSuccess)
+        ee = pq::fold_sorted<WW>(S.keys[0], S.coeffs[0], P.n0, S.keys[1], S.coeffs[1], head, &n_fold, scratch,
+                                 E->stream, &E->launches);
+      return ee;
+    });
+    if (e != cudaSuccess) return E->cuda_fail(e, "folding the observable");
+    S.cur = 1;
+    P.n0 = P.n_live = P.peak = n_fold;
+  } else if (P.n0) {
     cudaMemcpyAsync(S.keys[0], P.hk.data(), P.n0 * W * 8, cudaMemcpyHostToDevice, E->stream);
     cudaMemcpyAsync(S.coeffs[0], P.hc.data(), P.n0 * 8, cudaMemcpyHostToDevice, E->stream);
   }
@@ -1368,8 +1403,24 @@ int finalize(pq_engine* E, Slot& S, Plan& P, std::vector<pq::ExpectPartial>* par
         return 0;
       });
     }
-    cudaMemcpyAsync(S.out_keys.data(), S.keys[src], n_fin * W * 8, cudaMemcpyDeviceToHost, E->stream);
-    cudaMemcpyAsync(S.out_coeffs.data(), S.coeffs[src], n_fin * 8, cudaMemcpyDeviceToHost, E->stream);
+    const u64* out_k = S.keys[src];
+    const double* out_c = S.coeffs[src];
+    if (in.cfg->want_terms == 2) {  // in key order: the radix sort into the engine's sort buffer
+      const u64 sw = pq::sort_scratch_words(n_fin, W);
+      if ((e = E->sort_buf.ensure((sw + n_fin * (u64)(W + 1)) * 8)) != cudaSuccess)
+        return E->cuda_fail(e, "sort scratch");
+      u64* scratch = E->sort_buf.at<u64>(0);
+      u64* sk = scratch + sw;
+      double* sc = reinterpret_cast<double*>(sk + n_fin * W);
+      e = with_words(W, [&](auto w) {
+        return pq::sort_rows<decltype(w)::value>(out_k, out_c, n_fin, sk, sc, scratch, E->stream, &E->launches);
+      });
+      if (e != cudaSuccess) return E->cuda_fail(e, "sorting the terms");
+      out_k = sk;
+      out_c = sc;
+    }
+    cudaMemcpyAsync(S.out_keys.data(), out_k, n_fin * W * 8, cudaMemcpyDeviceToHost, E->stream);
+    cudaMemcpyAsync(S.out_coeffs.data(), out_c, n_fin * 8, cudaMemcpyDeviceToHost, E->stream);
   }
   return PQ_OK;
 }

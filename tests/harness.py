@@ -99,7 +99,7 @@ class GpuResult:
         self.res = res
 
 
-def make_cfg(p: Problem, want_terms=True, noise_plugin=None, truncator=None):
+def make_cfg(p: Problem, want_terms=True, noise_plugin=None, truncator=None, sort_terms=False):
     """The RunConfig of a problem and the arrays it points into."""
     cfg = _native.RunConfig()
     cfg.basis_kind = p.basis
@@ -120,12 +120,13 @@ def make_cfg(p: Problem, want_terms=True, noise_plugin=None, truncator=None):
     elif noise_plugin is not None:
         cfg.noise_kind, cfg.noise_plugin = _native.PQ_NOISE_PLUGIN, noise_plugin
     cfg.truncator = truncator
-    cfg.want_terms = 1 if want_terms else 0
+    cfg.want_terms = (2 if sort_terms else 1) if want_terms else 0
     return cfg, keep
 
 
-def run_gpu(engine, p: Problem, want_terms=True, noise_plugin=None, truncator=None) -> GpuResult:
-    cfg, keep = make_cfg(p, want_terms, noise_plugin, truncator)
+def run_gpu(engine, p: Problem, want_terms=True, noise_plugin=None, truncator=None, sort_terms=False) -> GpuResult:
+    """pq_run; sort_terms asks the engine for its final terms in key order."""
+    cfg, keep = make_cfg(p, want_terms, noise_plugin, truncator, sort_terms)
     res, nt = engine.run(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag)
     keys = coeffs = None
     if want_terms:
