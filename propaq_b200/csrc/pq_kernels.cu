@@ -69,27 +69,46 @@ struct Grp {
 // group arrives on the top counter, and the last top arrival releases
 // everyone by bumping the generation.  Every wait is bounded; once one
 // expires, ERR_BARRIER_TIMEOUT makes every later barrier fall through.
-// The three steps run on thread 0 of each block, after a fence.
+// The three steps run on thread 0 of each block, after the block's
+// __syncthreads; the arrivals are release-acquire atomics at GPU scope and
+// the wait an acquire load, so what any thread of any block wrote before the
+// barrier is visible to every thread after it, without a full fence.
+__device__ __forceinline__ u32 atom_add_acq_rel(u32* p, u32 v) {
+  u32 old;
+  asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ u32 ld_acquire(const u32* p) {
+  u32 v;
+  asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(u32* p, u32 v) {
+  asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
-// Arrives; true for the last arrival of the whole grid.
+// Arrives; true for the last arrival of the whole grid.  Grids of up to
+// BAR_FLAT blocks arrive on the top counter directly: one atomic round trip
+// instead of two, for at most BAR_FLAT atomics queued on one address.
+constexpr u32 BAR_FLAT = 320;
 __device__ __forceinline__ bool barrier_arrive(SweepState* st, const Grp g_) {
   const u32 nb = g_.nblk;
+  if (nb <= BAR_FLAT) return atom_add_acq_rel(&st->bar_count, 1u) == nb - 1;
   const u32 grp = g_.bid % BAR_GROUPS;
   const u32 in_grp = nb / BAR_GROUPS + (grp < nb % BAR_GROUPS ? 1u : 0u);
   const u32 n_grp = nb < BAR_GROUPS ? nb : BAR_GROUPS;
-  if (atomicAdd(&st->bar_group[grp].count, 1u) != in_grp - 1) return false;
-  st->bar_group[grp].count = 0;
-  return atomicAdd(&st->bar_count, 1u) == n_grp - 1;
+  if (atom_add_acq_rel(&st->bar_group[grp].count, 1u) != in_grp - 1) return false;
+  st->bar_group[grp].count = 0;  // no block arrives on it again before the release
+  return atom_add_acq_rel(&st->bar_count, 1u) == n_grp - 1;
 }
 __device__ __forceinline__ void barrier_release(SweepState* st, u32 g) {
   st->bar_count = 0;
-  __threadfence();
-  atomicExch(&st->bar_gen, g + 1);
+  st_release(&st->bar_gen, g + 1);  // orders the two resets and everything before it
 }
 __device__ __forceinline__ void barrier_wait(SweepState* st, u32 g) {
   const u32 limit = st->barrier_limit;  // set by the host for the launch
   u32 spins = 0;
-  while (*(volatile u32*)&st->bar_gen == g) {
+  while (ld_acquire(&st->bar_gen) == g) {
     if (*(volatile u32*)&st->error & ERR_BARRIER_TIMEOUT) break;
     if (++spins > limit) {
       atomicOr(&st->error, ERR_BARRIER_TIMEOUT);
@@ -102,13 +121,11 @@ __device__ __forceinline__ void barrier_wait(SweepState* st, u32 g) {
 __device__ __forceinline__ void grid_barrier(SweepState* st, u32& gen, const Grp g_) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
     if (barrier_arrive(st, g_))
       barrier_release(st, gen);
     else
       barrier_wait(st, gen);
     ++gen;
-    __threadfence();
   }
   __syncthreads();
 }
@@ -131,7 +148,6 @@ __device__ __forceinline__ void op_barrier(SweepState* st, u32& gen, const Grp g
                                            u32 n_extra, OpShared& os, Prefetch prefetch) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
     if (barrier_arrive(st, g_)) {
       barrier_release(st, gen);
       prefetch();
@@ -140,7 +156,6 @@ __device__ __forceinline__ void op_barrier(SweepState* st, u32& gen, const Grp g
       barrier_wait(st, gen);
     }
     ++gen;
-    __threadfence();
     const u64 n = ld_volatile(n_next);
     const u32 e = *(volatile u32*)&st->error;
     const u32 y = *(volatile u32*)&st->yield_after;
@@ -1032,33 +1047,65 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
 #include "pq_class.cuh"
 
 // Runs ops [a.op_begin, a.op_end) of one propagation on the blocks of `grp`.
+// 8-byte asynchronous copy global -> shared (cp.async; completes at cp_async_wait).
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  const u32 d = (u32)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <int W, int ALG>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   __shared__ TileSmem sm;
-  __shared__ GateDesc<W> sgs[4];  // the op's generator(s)
-  __shared__ OpDesc sod;
+  // The running op's descriptor and generator(s) in buffer sb; the next op's
+  // are copied into the other buffer while the running op works.
+  __shared__ __align__(16) GateDesc<W> sgs[2][4];
+  __shared__ __align__(8) OpDesc sod[2];
   __shared__ OpShared os;
   SweepState* st = a.st;
   u32 gen = *(volatile u32*)&st->bar_gen;
   int cur = (int)a.cur0;
   u32 op = a.op_begin;
+  u32 sb = 0;
   // The live count entering the next op is in n[par]; each op writes
   // n[par ^ 1].  (Not n[op & 1]: a fused op is several ops.)
   u32 par = op & 1u;
-  // Thread 0, once every thread is done with the op's shared descriptors.
-  auto fetch_op = [&](u32 k) {
+  const GateDesc<W>* gdesc = reinterpret_cast<const GateDesc<W>*>(a.gates);
+  auto rotation_op = [](u32 kind) {
+    return kind != OP_NOISE_SCALE && kind != OP_NOISE_COMPACT && !is_class(kind);
+  };
+  // Thread 0: op k's descriptors into buffer b, synchronously.
+  auto fetch_op = [&](u32 k, u32 b) {
     if (k >= a.op_end) return;
     const OpDesc d = a.ops[k];
-    sod = d;
-    const GateDesc<W>* gd = reinterpret_cast<const GateDesc<W>*>(a.gates);
-    if (d.kind != OP_NOISE_SCALE && d.kind != OP_NOISE_COMPACT && !is_class(d.kind))
-      for (u32 i = 0; i < fused_count(d.kind); ++i) sgs[i] = gd[d.idx + i];
+    sod[b] = d;
+    if (rotation_op(d.kind))
+      for (u32 i = 0; i < fused_count(d.kind); ++i) sgs[b][i] = gdesc[d.idx + i];
+  };
+  // Warp 0, at the start of an op: the copies of op k's descriptor and of the
+  // gate descriptors from gi on (those of the next rotation op -- gate
+  // descriptors are in op order) into buffer b.  Returns how many gate
+  // descriptors it copies.
+  auto prefetch_op = [&](u32 k, u32 gi, u32 b) -> u32 {
+    if (k >= a.op_end) return 0;
+    const u32 lane = threadIdx.x & 31;
+    if (lane == 0) cp_async8(&sod[b], a.ops + k);
+    const u32 ng = gi < a.n_gdesc ? (a.n_gdesc - gi < 4u ? a.n_gdesc - gi : 4u) : 0u;
+    constexpr u32 WORDS = sizeof(GateDesc<W>) / 8;
+    static_assert(sizeof(GateDesc<W>) % 8 == 0, "gate descriptors copy in 8-byte words");
+    const u64* src = reinterpret_cast<const u64*>(gdesc + gi);
+    u64* dst = reinterpret_cast<u64*>(&sgs[b][0]);
+    for (u32 w = lane; w < ng * WORDS; w += 32) cp_async8(dst + w, src + w);
+    return ng;
   };
   if (threadIdx.x == 0) {
-    fetch_op(op);
+    fetch_op(op, 0);
     os.n = ld_volatile(&st->n[par]);
     sm.rec_on = 0;
   }
+  u32 g_next = 0;  // warp 0: the gate descriptor the next rotation op is expected to start at
+  // Block 0, thread 0: the largest live count this launch has seen.
+  u64 peak = (grp.bid == 0 && threadIdx.x == 0) ? ld_volatile(&st->peak) : 0;
   // Adjoint recording: every block places the ops identically from the same
   // live counts, so the offsets agree without communication.
   u64 rb = a.rec_idx ? ld_volatile(&st->rec_next) : 0, rkb = a.rec_idx ? ld_volatile(&st->rec_key_next) : 0;
@@ -1076,7 +1123,8 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
   __syncthreads();
   bool stopped = false;  // a capacity stop inside a fused op
   while (op < a.op_end) {
-    OpDesc od = sod;
+    OpDesc od = sod[sb];
+    const GateDesc<W>* sg = sgs[sb];
     // A launch that resumes inside a fused group (after a capacity stop) runs
     // the remaining rotations as plain ones.
     if (od.kind == OP_GATE_TAIL) od.kind = OP_GATE;
@@ -1097,6 +1145,14 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
         st->grid_stop = 1;
       }
       break;
+    }
+    // The next op's descriptors, copied while this one runs: gate descriptors
+    // follow this op's (or stay where they were after a noise op).
+    u32 g_pred = 0, g_copied = 0;
+    if (threadIdx.x < 32) {
+      if (rotation_op(od.kind) || is_class(od.kind)) g_next = od.idx + nops;
+      g_pred = g_next;
+      g_copied = prefetch_op(op + nops, g_pred, sb ^ 1u);
     }
     if (a.rec_idx) {
       const bool rec_op = gate_like || od.kind == OP_NOISE_COMPACT;
@@ -1120,9 +1176,9 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     }
     if (gate_like) {
       if (od.kind == OP_GATE) {
-        gate_op<W, ALG>(a, sgs[0], op, N, keys, coeffs, sm, grp, n_out);
+        gate_op<W, ALG>(a, sg[0], op, N, keys, coeffs, sm, grp, n_out);
       } else if (od.kind == OP_PHASE) {
-        phase_op<W, ALG>(a, sgs[0], op, N, keys, coeffs, sm, grp);
+        phase_op<W, ALG>(a, sg[0], op, N, keys, coeffs, sm, grp);
         if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, N);
       } else if (N == 0) {
         if (grp.bid == 0 && threadIdx.x == 0) st_volatile(n_out, 0);
@@ -1139,7 +1195,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
         }
         // rc 1: a device error; the barrier below ends the sweep
       } else if (nops == 2 && N <= (u64)grp.nblk * BLOCK * GATE2_TILES_PER_BLOCK && 4 * N <= a.cap) {
-        gate2_tiles<W, ALG>(a, sgs[0], sgs[1], op, N, keys, coeffs, sm, grp, n_out);
+        gate2_tiles<W, ALG>(a, sg[0], sg[1], op, N, keys, coeffs, sm, grp, n_out);
       } else {  // many rows: the rotations one after the other (op + i is rotation i's slot)
         split = true;
         u64 Ni = N;
@@ -1148,14 +1204,14 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
             if (grp.bid == 0 && threadIdx.x == 0) {
               st->n[par] = Ni;  // read as the next op's count (nobody reads n[par] during this op)
               st->halt = op + i;
-              if (Ni > st->peak) st->peak = Ni;
+              if (Ni > peak) peak = Ni;
             }
             op += i;
             stopped = true;
             break;
           }
           u64* out_i = i + 1 == nops ? n_out : &st->n_mid[i & 1];
-          gate_op<W, ALG>(a, sgs[i], op + i, Ni, keys, coeffs, sm, grp, out_i);
+          gate_op<W, ALG>(a, sg[i], op + i, Ni, keys, coeffs, sm, grp, out_i);
           if (i + 1 < nops) {
             grid_barrier(st, gen, grp);
             Ni = ld_volatile(out_i);
@@ -1183,30 +1239,48 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     if (a.idle_blocks && grp.bid == 0 && threadIdx.x == 0 && *(volatile u32*)a.idle_blocks >= a.yield_at)
       *(volatile u32*)&st->yield_after = op + 1;
     const bool cls = is_class(od.kind) && !split;
-    op_barrier(st, gen, grp, n_out, nops > 1 && !split && !cls ? a.tickets + op : nullptr, nops - 1, os,
-               [&] { fetch_op(op + nops); });
+    if (threadIdx.x < 32) cp_async_wait();  // the next op's descriptors, before the barrier's __syncthreads
+    // After the release, thread 0 checks the copied descriptor: a rotation op
+    // whose gate descriptors are not the ones copied is fetched again.
+    op_barrier(st, gen, grp, n_out, nops > 1 && !split && !cls ? a.tickets + op : nullptr, nops - 1, os, [&] {
+      const u32 k = op + nops;
+      if (k >= a.op_end) return;
+      const OpDesc d = sod[sb ^ 1u];
+      if (rotation_op(d.kind) && (d.idx != g_pred || fused_count(d.kind) > g_copied)) fetch_op(k, sb ^ 1u);
+    });
     par ^= 1u;
     if (os.err) {
       op += nops;
       break;
     }
+    if (grp.bid == 0 && cls && threadIdx.x < 32) {
+      // Counts after each rotation of the class but the last: the rows each
+      // one created (tickets), summed over the class by a warp scan.
+      u64 acc = N;
+      for (u32 i0 = 0; i0 + 1 < nops; i0 += 32) {
+        const u32 i = i0 + threadIdx.x;
+        const u64 v = i + 1 < nops ? (u64)__ldcg(a.tickets + op + i) : 0ull;
+        u64 inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const u64 y = __shfl_up_sync(FULL, inc, o);
+          if ((int)threadIdx.x >= o) inc += y;
+        }
+        if (i + 1 < nops) a.hist[op + i] = acc + inc;
+        acc += __shfl_sync(FULL, inc, 31);
+      }
+    }
     if (grp.bid == 0 && threadIdx.x == 0) {
       const u64 n_new = os.n;
       a.hist[op + nops - 1] = n_new;
-      if (cls) {  // counts after each rotation of the class: the rows each one created
-        u64 acc = N;
-        for (u32 i = 0; i + 1 < nops; ++i) {
-          acc += *(volatile u32*)(a.tickets + op + i);
-          a.hist[op + i] = acc;
-        }
-      } else if (nops > 1 && !split) {  // counts after each rotation of the group but the last
+      if (nops > 1 && !split && !cls) {  // counts after each rotation of the group but the last
         u64 acc = N;
         for (u32 i = 0; i + 1 < nops; ++i) {
           acc += os.extra[i];
           a.hist[op + i] = acc;
         }
       }
-      if (n_new > st->peak) st->peak = n_new;
+      if (n_new > peak) peak = n_new;
       if (a.stamps) {
         u64 t;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -1215,9 +1289,12 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
     }
     const bool stop = a.idle_blocks && os.yield_after == op + 1;
     op += nops;
+    sb ^= 1u;
     if (stop) break;
   }
+  if (threadIdx.x < 32) cp_async_wait();  // copies of an op the sweep stopped before
   if (grp.bid == 0 && threadIdx.x == 0) {
+    if (peak > st->peak) st->peak = peak;
     st->cur = (u32)cur;
     st->end_op = op;
     if (a.rec_idx) {

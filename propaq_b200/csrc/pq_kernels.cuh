@@ -76,7 +76,9 @@ struct SweepState {
 
 struct SweepArgs {
   const OpDesc* ops;
-  const void* gates;       // GateDesc<W>[]
+  const void* gates;       // GateDesc<W>[], in op order
+  u32 n_gdesc;             // gate descriptors in `gates`
+  u32 pad0_;
   const double* tables;    // noise factor tables, table_len entries each
   u32 table_len;
   u32 n_units;
