@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="sweep blocks per SM (0 = by live count; batch: as many as fit)")
+    ap.add_argument("--fuse-max", type=int, default=0, help="rotations fused into one pass, 1-4 (0 = the engine's 4)")
+    ap.add_argument("--tile-items", type=int, default=0, help="rows per thread of a many-row gate tile, 1-4 (0 = 4)")
+    ap.add_argument("--bucket-slots", type=int, default=0, help="hash-table bucket width: 2, 4 or 8 (0 = 4)")
     ap.add_argument("--split", type=int, default=1, help="batch: 0 equal grid shares, 1 by remaining work")
     ap.add_argument("--rebalance-pct", type=int, default=25, help="batch: re-split when this %% of the grid idles")
     ap.add_argument("--no-sequential", action="store_true", help="batch: skip the sequential pq_run comparison")
@@ -301,9 +304,11 @@ def main_batch(args, world, rank, local):
     for p in probs:
         cfg, k = make_cfg(p, want_terms=False)
         cfg.blocks_per_sm = args.blocks_per_sm
+        cfg.fuse_max, cfg.tile_items, cfg.bucket_slots = args.fuse_max, args.tile_items, args.bucket_slots
         keep.append(k)
         items.append((cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag))
-    tune = dict(blocks_per_sm=args.blocks_per_sm, split=args.split, rebalance_pct=args.rebalance_pct)
+    tune = dict(blocks_per_sm=args.blocks_per_sm, split=args.split, rebalance_pct=args.rebalance_pct,
+                fuse_max=args.fuse_max, tile_items=args.tile_items, bucket_slots=args.bucket_slots)
     jobs = [(PauliPropagator(noise=w.noise(), truncation=w.truncation(), device=local), w.observable, w.circuit,
              w.initial_state) for w in wls]
     WM = max(p.n_words for p in probs)
@@ -318,7 +323,7 @@ def main_batch(args, world, rank, local):
         engine.run_batch(items, **tune)
     tuned = None
     if not args.no_autotune:
-        # The project's autotuner picks the launch parameters by measurement
+        # The project's autotuner picks the launch and kernel parameters by measurement
         # (propaq_b200.tuning), once per batch shape, before the timed region.
         from propaq_b200.tuning import batch_signature, default_tuner
 
@@ -673,6 +678,7 @@ def main():
         cfg.noise_kind, cfg.noise_tables, cfg.noise_table_len = _native.PQ_NOISE_TABLE, table.ctypes.data, len(table)
     cfg.want_terms = 0
     cfg.blocks_per_sm = args.blocks_per_sm
+    cfg.fuse_max, cfg.tile_items, cfg.bucket_slots = args.fuse_max, args.tile_items, args.bucket_slots
 
     def device_step():
         return engine.run(cfg, prob.obs_keys, prob.obs_coeffs, prob.gate_keys, prob.angles, prob.offsets, prob.diag)

@@ -90,6 +90,13 @@ typedef struct pq_run_config {
   uint32_t log_gates;        /* keep per-gate records for pq_result_gates (the
                                 Logger's verbose log); rotations then run one op
                                 each, unfused, so each has its own device time  */
+  /* Tuning; 0 = the engine's default.  Results do not depend on them. */
+  uint32_t fuse_max;         /* consecutive commuting rotations run in one pass
+                                over the rows: 1-2 (default 2)                  */
+  uint32_t tile_items;       /* rows per thread of a many-row gate tile: 1-4
+                                (default 4)                                     */
+  uint32_t bucket_slots;     /* hash-table slots a key's probe starts in: 2, 4
+                                or 8 (default 4)                                */
 } pq_run_config;
 
 /* crates/core/src/interface/results.rs:8-51 (PropagationResult), plus the
@@ -233,6 +240,10 @@ typedef struct pq_batch_tuning {
   uint32_t rebalance_pct;  /* when this % of the grid has been left by finished
                               instances, the others stop at their next op and
                               the grid is re-split among them; 0 = never        */
+  uint32_t fuse_max;       /* as pq_run_config, for every instance; 0 = each
+                              instance's own                                    */
+  uint32_t tile_items;
+  uint32_t bucket_slots;
 } pq_batch_tuning;
 
 /* Runs n independent propagations of one basis in shared persistent

@@ -51,6 +51,9 @@ class RunConfig(ctypes.Structure):
         ("want_terms", ctypes.c_uint32),
         ("blocks_per_sm", ctypes.c_uint32),
         ("log_gates", ctypes.c_uint32),
+        ("fuse_max", ctypes.c_uint32),
+        ("tile_items", ctypes.c_uint32),
+        ("bucket_slots", ctypes.c_uint32),
     ]
 
 
@@ -136,7 +139,8 @@ class EngineLimits(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     """pq_batch_tuning."""
 
-    _fields_ = [("blocks_per_sm", ctypes.c_uint32), ("split", ctypes.c_uint32), ("rebalance_pct", ctypes.c_uint32)]
+    _fields_ = [("blocks_per_sm", ctypes.c_uint32), ("split", ctypes.c_uint32), ("rebalance_pct", ctypes.c_uint32),
+                ("fuse_max", ctypes.c_uint32), ("tile_items", ctypes.c_uint32), ("bucket_slots", ctypes.c_uint32)]
 
 
 NOISE_FACTOR_FN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64),
@@ -281,10 +285,11 @@ class Engine:
         return res, nt, grad
 
     def run_batch(self, items, blocks_per_sm: int = 0, split: int = 1, rebalance_pct: int = 25,
-                  want_n_terms: bool = True):
+                  want_n_terms: bool = True, fuse_max: int = 0, tile_items: int = 0, bucket_slots: int = 0):
         """Runs pq_run_batch on a list of (cfg, obs_words, obs_coeffs, gate_words,
         gate_angles, layer_offsets, diag_state) tuples; returns one
-        (RunResult, n_terms array or None) per instance."""
+        (RunResult, n_terms array or None) per instance.  fuse_max, tile_items
+        and bucket_slots (0 = each instance's own) tune every instance."""
         keep = []
         insts = (Instance * len(items))()
         out = []
@@ -307,7 +312,7 @@ class Engine:
             inst.result = ctypes.pointer(res)
             out.append((res, nt))
         with self.lock:
-            tune = BatchTuning(blocks_per_sm, split, rebalance_pct)
+            tune = BatchTuning(blocks_per_sm, split, rebalance_pct, fuse_max, tile_items, bucket_slots)
             rc = lib().pq_run_batch(self._h, insts, len(items), ctypes.byref(tune))
             if rc != PQ_OK:
                 raise_for(rc, lib().pq_engine_last_error(self._h).decode(errors="replace"))

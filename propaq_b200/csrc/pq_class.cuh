@@ -173,7 +173,7 @@ __device__ bool run_lone(const ClassRules<W, ALG>& R, const u64* key0, const int
         if (row < a.cap) {
           store_key<W>(keys, row, key);
           coeffs[row] = cur.c;
-          insert<W>(key, row, a.table, a.table_mask, &a.st->error);
+          insert<W>(key, row, a.table, a.table_mask, a.table_bmask, &a.st->error);
         } else {
           atomicOr(&a.st->error, ERR_CAPACITY);
         }
@@ -227,7 +227,7 @@ __device__ __noinline__ void run_warp_family(const ClassRules<W, ALG>& R, const 
     member_key<W>(rep, cg, sidx, c, q);
     double cj = 0.0;
     u64 es = NO_SLOT;
-    const long long j = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.st, cj, es);
+    const long long j = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, a.st, cj, es);
     if (j >= 0) {
       F.pres |= 1u << s;
       F.cf[s] = cj;
@@ -311,7 +311,7 @@ __device__ __forceinline__ void write_warp_family(const SweepArgs& a, const u64*
         store_key<W>(keys, row, q);
         coeffs[row] = F.cf[s];
         place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | (row & 0xffffffffULL), F.slot[s], a.table,
-                      a.table_mask, &a.st->error);
+                      a.table_mask, a.table_bmask, &a.st->error);
       } else {
         atomicOr(&a.st->error, ERR_CAPACITY);
       }
@@ -373,7 +373,7 @@ __device__ __noinline__ void class_phase_a(const SweepArgs& a, const GateDesc<W>
     const u64 h = key_hash<W>(rep);
     const u32 fp = (u32)(h >> 32);
     const u64 want = ((u64)fp << 32) | (u32)r;
-    u64 i = bucket_start(h, a.table_mask);
+    u64 i = (h & a.table_mask) & ~3ULL;  // buckets of 4 slots
     u64 found = NO_SLOT;
     for (u64 probe = 0; probe <= a.table_mask; ++probe) {
       u64 s = __ldcg(a.fam_table + i);

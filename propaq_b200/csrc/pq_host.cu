@@ -210,6 +210,7 @@ struct Slot {
   double* coeffs[2] = {nullptr, nullptr};
   u64* table = nullptr;
   u64 tcap = 0;
+  u64 bmask = ~3ULL;  // ~(slots per table bucket - 1) of the run the slot holds
   u64* status = nullptr;
   u64 cap = 0;
   int W = 0;
@@ -482,7 +483,7 @@ struct pq_engine {
   int rebuild_table(Slot& S, u64 n) {
     cudaMemsetAsync(S.table, 0xff, S.tcap * 8, stream);
     const cudaError_t e = with_words(S.W, [&](auto w) {
-      return pq::launch_rebuild<decltype(w)::value>(S.keys[S.cur], n, S.table, S.tcap - 1, d_err, stream);
+      return pq::launch_rebuild<decltype(w)::value>(S.keys[S.cur], n, S.table, S.tcap - 1, S.bmask, d_err, stream);
     });
     if (n) ++launches;
     if (e != cudaSuccess) return cuda_fail(e, "rebuild launch");
@@ -559,6 +560,8 @@ struct Inputs {
 // op sequence with its gate descriptors, the Clifford frame, and how far the
 // device has run it.  W is the width the device runs it at (>= in_words; the
 // extra words are zero).
+constexpr u32 FUSE_DEFAULT = 2;  // rotations a fused group holds unless the run says otherwise
+
 struct Plan {
   const Inputs* in = nullptr;
   int W = 1, alg = 0;
@@ -580,6 +583,10 @@ struct Plan {
   bool defer = true;
   bool log = false;  // per-gate records for the verbose log (pq_run_config::log_gates)
   bool has_class = false;  // some op is a class (fuse_classes)
+  // Tuning (pq_run_config / pq_batch_tuning): rotations fused into one pass,
+  // rows per thread of a many-row gate tile (0 = the kernel's 4), slots per
+  // table bucket.
+  u32 fuse_max = FUSE_DEFAULT, tile_items = 0, bucket_slots = 4;
   bool fold_on_device = false;  // hk / hc hold the admitted terms unfolded (DEVICE_FOLD_MIN)
   std::vector<u64> hk;
   std::vector<double> hc;
@@ -624,6 +631,9 @@ int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
   P.ccut = cfg->min_coeff;
   P.has_floor = cfg->min_terms >= 0;
   P.log = cfg->log_gates != 0;
+  P.fuse_max = cfg->fuse_max ? cfg->fuse_max : FUSE_DEFAULT;
+  P.tile_items = cfg->tile_items;
+  P.bucket_slots = cfg->bucket_slots ? cfg->bucket_slots : 4;
   P.floor_terms = P.has_floor ? (u64)cfg->min_terms : 0;
   const Plugin* np = reinterpret_cast<const Plugin*>(cfg->noise_plugin);
   P.tlen = cfg->noise_table_len ? cfg->noise_table_len : (size_t)P.n_units + 1;
@@ -714,6 +724,7 @@ int prepare(pq_engine* E, Plan& P, const Inputs& in, int W) {
 int setup_slot(pq_engine* E, Slot& S, Plan& P) {
   cudaError_t e;
   const int W = P.W;
+  S.bmask = ~(u64)(P.bucket_slots - 1);
   const u64 want_cap = next_pow2(std::max<u64>(4 * P.n0, 1ULL << 16));
   if (S.W != W || S.cap < want_cap) {
     if (int rc = E->resize(S, std::max(want_cap, S.W == W ? S.cap : 0), 0, S.cur, W)) return rc;
@@ -915,20 +926,22 @@ void fuse_classes(Plan& P) {
   }
 }
 
-// Marks runs of up to FUSE_MAX consecutive rotation ops whose
-// (frame-conjugated) generators pairwise commute and are independent (no
-// subset multiplies to the identity, so a family's members are distinct) as
-// fused groups: a head OP_GATE2 / 3 / 4 and OP_GATE_TAIL ops.  The sweep runs
-// a pair in one pass (gate2_tiles) and larger groups one rotation after the
-// other.  Pairs only: a measured one-pass kernel for 3 and 4 rotations (families
-// of 8 and 16 keys) was slower than pairs on every workload (kicked Ising
-// 46.6 and 52.4 ms against 42.0 ms), its per-family work outweighing the
-// barriers it saves.  Not with a TermBudget floor:
-// its lossless switch reads the live count between rotations; not when the
-// host decides branches; and the adjoint's runs do not fuse (each rotation
-// needs its own record).
-constexpr size_t FUSE_MAX = 2;
+// Marks runs of up to fuse_max (1 or 2, default 2) consecutive rotation ops
+// whose (frame-conjugated) generators pairwise commute and are independent
+// (no subset multiplies to the identity, so a family's members are distinct)
+// as fused groups: a head OP_GATE2 and an OP_GATE_TAIL op.  The sweep runs a
+// pair in one pass (gate2_tiles) while every block has at most a few tiles,
+// else one rotation after the other.  Pairs only: one-pass kernels for 3 and
+// 4 rotations were slower on every workload measured -- first with families
+// of 8 and 16 keys in registers (kicked Ising 10x10 x 20 steps 46.6 and 52.4
+// ms against 42.0 ms), then with each row's family over only the rotations it
+// anticommutes with (28.4 ms for groups of 4 against 23.4 ms for pairs, the
+// RX layers 19.2 against 14.4 ms): their per-family work outweighs the
+// barriers they save.  Not with a TermBudget floor: its lossless switch reads
+// the live count between rotations; not when the host decides branches; and
+// the adjoint's runs do not fuse (each rotation needs its own record).
 void fuse_groups(Plan& P) {
+  const size_t FUSE_MAX = std::min<size_t>(P.fuse_max, pq::GROUP_MAX);
   if (P.has_floor || P.host_ops || P.log) return;
   const size_t gw = gdesc_words(P.W);
   const int W = P.W;
@@ -1033,6 +1046,8 @@ pq::SweepArgs sweep_args(Slot& S, const Plan& P, pq::SweepState* st, u32 blk_beg
   }
   a.table = S.table;
   a.table_mask = S.tcap - 1;
+  a.table_bmask = S.bmask;
+  a.tile_items = P.tile_items;
   a.cap = S.cap;
   a.status = S.status;
   a.tickets = S.tickets;
@@ -1863,6 +1878,9 @@ int run_batch(pq_engine* E, const std::vector<Inputs>& ins, int WM, const pq_bat
     if (int rc = prepare(E, plans[i], ins[i], W)) return rc;
     if (plans[i].host_ops)
       return E->fail(PQ_ERR_UNSUPPORTED, "a batch does not run truncator plugins or key-reading noise; use pq_run");
+    if (tune.fuse_max) plans[i].fuse_max = tune.fuse_max;
+    if (tune.tile_items) plans[i].tile_items = tune.tile_items;
+    if (tune.bucket_slots) plans[i].bucket_slots = tune.bucket_slots;
     if (int rc = setup_slot(E, E->slots[i], plans[i])) return rc;
     if (int rc = build_ops(plans[i], no_sync)) return rc;
     fuse_classes(plans[i]);
@@ -2009,6 +2027,10 @@ int check_inputs(pq_engine* E, const pq_run_config* cfg, size_t ng, const uint32
   if (!W)
     return E->fail(PQ_ERR_INVALID, "propaq: " + std::to_string(cfg->n_units) +
                                        " units exceeds the engine's maximum of 2048");
+  if (cfg->fuse_max > pq::GROUP_MAX) return E->fail(PQ_ERR_INVALID, "fuse_max must be 0..2");
+  if (cfg->tile_items > 4) return E->fail(PQ_ERR_INVALID, "tile_items must be 0..4");
+  if (cfg->bucket_slots != 0 && cfg->bucket_slots != 2 && cfg->bucket_slots != 4 && cfg->bucket_slots != 8)
+    return E->fail(PQ_ERR_INVALID, "bucket_slots must be 0, 2, 4 or 8");
   if (nl && (!lo || lo[0] != 0 || lo[nl] != ng)) return E->fail(PQ_ERR_INVALID, "layer offsets do not cover the gates");
   if (!nl && ng) return E->fail(PQ_ERR_INVALID, "layer offsets do not cover the gates");
   for (size_t l = 0; l < nl; ++l)
@@ -2045,8 +2067,12 @@ int pq_run_batch(pq_engine* E, const pq_instance* insts, size_t n, const pq_batc
   BudgetScope scope(E ? &E->budget : nullptr);
   if (!E || !insts || !n) return PQ_ERR_INVALID;
   E->err.clear();
-  const pq_batch_tuning tune = tuning ? *tuning : pq_batch_tuning{0, 1, 25};
+  const pq_batch_tuning tune = tuning ? *tuning : pq_batch_tuning{0, 1, 25, 0, 0, 0};
   if (tune.split > 1) return E->fail(PQ_ERR_INVALID, "split must be 0 (equal) or 1 (by remaining work)");
+  if (tune.fuse_max > pq::GROUP_MAX) return E->fail(PQ_ERR_INVALID, "fuse_max must be 0..2");
+  if (tune.tile_items > 4) return E->fail(PQ_ERR_INVALID, "tile_items must be 0..4");
+  if (tune.bucket_slots != 0 && tune.bucket_slots != 2 && tune.bucket_slots != 4 && tune.bucket_slots != 8)
+    return E->fail(PQ_ERR_INVALID, "bucket_slots must be 0, 2, 4 or 8");
   if (tune.rebalance_pct > 100) return E->fail(PQ_ERR_INVALID, "rebalance_pct must be 0..100");
   const uint32_t basis = insts[0].cfg.basis_kind;
   int WM = 1;

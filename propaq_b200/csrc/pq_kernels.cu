@@ -49,6 +49,7 @@ constexpr u32 BAR_GROUPS = SweepState::BAR_GROUPS;
 // A fused op runs both rotations in one pass while each block has at most
 // this many tiles of rows; above, one after the other.
 constexpr u32 GATE2_TILES_PER_BLOCK = 4;
+static_assert(GROUP_MAX == 2, "the sweep runs fused pairs (gate2_tiles)");
 
 enum : int { S_EMIT = 0, S_HELD = 1, S_DROP = 2 };
 
@@ -244,11 +245,13 @@ __device__ __forceinline__ void store_key(u64* keys, u64 row, const u64* k) {
   }
 }
 
-// The table is linear-probed from a bucket of 4 slots (one 32-byte sector):
-// a lookup starts at the first slot of the key's bucket and scans forward
-// until it meets the key or an empty slot; an insert takes the first empty
-// slot of the same sequence.
-__device__ __forceinline__ u64 bucket_start(u64 h, u64 mask) { return (h & mask) & ~3ULL; }
+// The table is linear-probed from a bucket of 2, 4 or 8 slots (bmask = ~(slots
+// - 1); 4 slots are one 32-byte sector): a lookup starts at the first slot of
+// the key's bucket and scans forward until it meets the key or an empty slot;
+// an insert takes the first empty slot of the same sequence.  The first probe
+// loads 4 slots, so a bucket of 2 may span two sectors and one of 8 takes two
+// probes when its first half is full.
+__device__ __forceinline__ u64 bucket_start(u64 h, u64 mask, u64 bmask) { return (h & mask) & bmask; }
 
 // Continues a lookup of q from slot i (see bucket_start).  Rows the running
 // gate appends (>= n_pre) are skipped: no lookup of this gate can target them.
@@ -273,10 +276,10 @@ __device__ long long lookup_from(const u64* q, u32 fp, u64 i, u64 n_pre, const u
 }
 
 template <int W>
-__device__ void insert(const u64* q, u64 row, u64* table, u64 mask, u32* error) {
+__device__ void insert(const u64* q, u64 row, u64* table, u64 mask, u64 bmask, u32* error) {
   const u64 h = key_hash<W>(q);
   const u64 v = ((h >> 32) << 32) | (row & 0xffffffffULL);
-  u64 i = bucket_start(h, mask);
+  u64 i = bucket_start(h, mask, bmask);
   for (u64 probe = 0; probe <= mask; ++probe) {
     if (__ldcg(table + i) == EMPTY_SLOT && atomicCAS(table + i, EMPTY_SLOT, v) == EMPTY_SLOT) return;
     i = (i + 1) & mask;
@@ -292,10 +295,10 @@ __device__ void insert(const u64* q, u64 row, u64* table, u64 mask, u32* error) 
 constexpr u32 PENDING_ROW = 0xfffffffeu;
 constexpr u64 NO_SLOT = ~0ULL;
 template <int W>
-__device__ u64 claim_slot(const u64* q, u64* table, u64 mask, u32* error) {
+__device__ u64 claim_slot(const u64* q, u64* table, u64 mask, u64 bmask, u32* error) {
   const u64 h = key_hash<W>(q);
   const u64 v = ((h >> 32) << 32) | PENDING_ROW;
-  u64 i = bucket_start(h, mask);
+  u64 i = bucket_start(h, mask, bmask);
   for (u64 probe = 0; probe <= mask; ++probe) {
     if (__ldcg(table + i) == EMPTY_SLOT && atomicCAS(table + i, EMPTY_SLOT, v) == EMPTY_SLOT) return i;
     i = (i + 1) & mask;
@@ -312,12 +315,14 @@ __device__ __forceinline__ void set_row(u64* table, u64 slot, u64 row) {
 // key on a fingerprint match).
 template <int W>
 __device__ __forceinline__ long long lookup(const u64* q, u64 n_pre, const u64* keys, const u64* table, u64 mask,
-                                            SweepState* st) {
+                                            u64 bmask, SweepState* st) {
   const u64 h = key_hash<W>(q);
   const u32 fp = (u32)(h >> 32);
-  const u64 b = bucket_start(h, mask);
-  const ulonglong2* bp = reinterpret_cast<const ulonglong2*>(table + b);
-  const ulonglong2 s01 = __ldcg(bp), s23 = __ldcg(bp + 1);
+  const u64 b = bucket_start(h, mask, bmask);
+  // slots b, b + 1 and the next two on the probe sequence (wrapping: a
+  // bucket of 2 may be the table's last)
+  const ulonglong2 s01 = __ldcg(reinterpret_cast<const ulonglong2*>(table + b));
+  const ulonglong2 s23 = __ldcg(reinterpret_cast<const ulonglong2*>(table + ((b + 2) & mask)));
   const u64 sl[4] = {s01.x, s01.y, s23.x, s23.y};
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
@@ -369,17 +374,20 @@ __device__ long long lookup_from_c(const u64* q, u32 fp, u64 i, u64 n_pre, const
 }
 template <int W>
 __device__ __forceinline__ long long lookup_c(const u64* q, u64 n_pre, const u64* keys, const double* coeffs,
-                                              const u64* table, u64 mask, SweepState* st, double& cj, u64& empty) {
+                                              const u64* table, u64 mask, u64 bmask, SweepState* st, double& cj,
+                                              u64& empty) {
   const u64 h = key_hash<W>(q);
   const u32 fp = (u32)(h >> 32);
-  const u64 b = bucket_start(h, mask);
-  const ulonglong2* bp = reinterpret_cast<const ulonglong2*>(table + b);
-  const ulonglong2 s01 = __ldcg(bp), s23 = __ldcg(bp + 1);
+  const u64 b = bucket_start(h, mask, bmask);
+  // slots b, b + 1 and the next two on the probe sequence (wrapping: a
+  // bucket of 2 may be the table's last)
+  const ulonglong2 s01 = __ldcg(reinterpret_cast<const ulonglong2*>(table + b));
+  const ulonglong2 s23 = __ldcg(reinterpret_cast<const ulonglong2*>(table + ((b + 2) & mask)));
   const u64 sl[4] = {s01.x, s01.y, s23.x, s23.y};
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
     if (sl[m] == EMPTY_SLOT) {
-      empty = b + m;
+      empty = (b + m) & mask;
       return -1;
     }
     const u32 row = (u32)sl[m];
@@ -403,13 +411,13 @@ __device__ __forceinline__ long long lookup_c(const u64* q, u64 n_pre, const u64
 // before it; if another key took the slot meanwhile, the probe goes on as in
 // insert.  Returns the slot, or NO_SLOT if the table is full.
 template <int W>
-__device__ u64 place_from(const u64* q, u64 v, u64 start, u64* table, u64 mask, u32* error) {
+__device__ u64 place_from(const u64* q, u64 v, u64 start, u64* table, u64 mask, u64 bmask, u32* error) {
   u64 i;
   if (start != NO_SLOT) {
     if (atomicCAS(table + start, EMPTY_SLOT, v) == EMPTY_SLOT) return start;
     i = (start + 1) & mask;
   } else {
-    i = bucket_start(key_hash<W>(q), mask);
+    i = bucket_start(key_hash<W>(q), mask, bmask);
   }
   for (u64 probe = 0; probe <= mask; ++probe) {
     if (__ldcg(table + i) == EMPTY_SLOT && atomicCAS(table + i, EMPTY_SLOT, v) == EMPTY_SLOT) return i;
@@ -568,7 +576,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
       u64 q[W];
 #pragma unroll
       for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ g.gen[w];
-      j[k] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cj[k], es[k]);
+      j[k] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cj[k], es[k]);
     }
     // The lower row of a pair owns both coefficients.
     u32 own = 0;
@@ -596,7 +604,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
         if (si == S_EMIT) {
           emit |= 1u << k;
           bval[k] = bi;
-          slot[k] = place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | PENDING_ROW, es[k], a.table, a.table_mask,
+          slot[k] = place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | PENDING_ROW, es[k], a.table, a.table_mask, a.table_bmask,
                                   &st->error);
         }
         if (sm.rec_on) record_single(a, sm, r, c[k]);
@@ -645,14 +653,16 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
   if (lane == 0 && n_anti && a.anti) atomicAdd(a.anti + op, (u64)n_anti);
 }
 
-// Many rows: 1024-row tiles handed out in order by a per-op ticket, each
-// thread taking its MAX_ITEMS rows one after the other.
+// Many rows: tiles of `its` x BLOCK rows (its = SweepArgs::tile_items, 1 to
+// MAX_ITEMS) handed out in order by a per-op ticket, each thread taking its
+// rows one after the other.
 template <int W, int ALG>
 __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc<W>& d, u32 op, u64 N, u64* keys,
                                                  double* coeffs, TileSmem& sm, u64* n_out) {
   using Ops = typename Alg<ALG>::T;
   constexpr int IT = MAX_ITEMS;
-  constexpr int TL = BLOCK * IT;
+  const u32 its = a.tile_items && a.tile_items < (u32)IT ? a.tile_items : (u32)IT;
+  const u64 TL = (u64)BLOCK * its;
   SweepState* st = a.st;
   const u32 ntiles = (u32)((N + TL - 1) / TL);
   const bool lossless = a.min_terms && N < a.min_terms;
@@ -681,7 +691,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
     for (int k = 0; k < IT; ++k) {
       bval[k] = 0.0;
       const u64 r = (u64)t * TL + (u64)k * BLOCK + threadIdx.x;
-      if (r >= N) continue;
+      if ((u32)k >= its || r >= N) continue;
       u64 key[W];
       load_key<W>(keys, r, key);
       if (!Ops::template anticommutes<W>(g, key)) continue;
@@ -692,7 +702,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
       for (int w = 0; w < W; ++w) q[w] = key[w] ^ g.gen[w];
       double cj = 0.0;
       u64 es = NO_SLOT;
-      const long long j = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cj, es);
+      const long long j = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cj, es);
       if (j >= 0 && (u64)j < r) continue;  // the lower row of the pair owns it
       const double bi = __dmul_rn(__dmul_rn(c, sn), neg_im(Ops::template product_exp<W>(g, key), g.sign));
       const int si = a.host_state ? (int)a.host_state[r] : state(c, q);
@@ -741,7 +751,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
       for (int w = 0; w < W; ++w) q[w] ^= g.gen[w];
       store_key<W>(keys, row, q);
       coeffs[row] = bval[k];
-      place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | (row & 0xffffffffULL), eslot[k], a.table, a.table_mask,
+      place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | (row & 0xffffffffULL), eslot[k], a.table, a.table_mask, a.table_bmask,
                     &st->error);
       if (sm.rec_on) a.rec_idx[sm.rec_base + r] = (u32)row;
     }
@@ -823,15 +833,15 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
       u64 q[W];
       if (a1) {
         member(1, q);
-        j[1] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cm[1], es[1]);
+        j[1] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cm[1], es[1]);
       }
       if (a2) {
         member(2, q);
-        j[2] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cm[2], es[2]);
+        j[2] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cm[2], es[2]);
       }
       if (a1 && a2) {
         member(3, q);
-        j[3] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, st, cm[3], es[3]);
+        j[3] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cm[3], es[3]);
       }
     }
     const bool own = (a1 || a2) && (j[1] < 0 || (u64)j[1] > r) && (j[2] < 0 || (u64)j[2] > r) &&
@@ -906,7 +916,7 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
         u64 q[W];
         member(m, q);
         // before the scan: see claim_slot
-        slot[m - 1] = place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | PENDING_ROW, es[m], a.table, a.table_mask,
+        slot[m - 1] = place_from<W>(q, ((key_hash<W>(q) >> 32) << 32) | PENDING_ROW, es[m], a.table, a.table_mask, a.table_bmask,
                                     &st->error);
         if (born[m] == 1) {
           ++n_born1;
@@ -1022,7 +1032,7 @@ __device__ __noinline__ void noise_compact_op(const SweepArgs& a, const double* 
                                   : (a.max_weight == NO_WEIGHT_CUT || w <= a.max_weight) &&
                                         (!a.has_min_coeff || fabs(c) >= a.min_coeff);
       keep |= (u32)kp << k;
-      if (kp) slot[k] = claim_slot<W>(key[k], a.table, a.table_mask, &st->error);
+      if (kp) slot[k] = claim_slot<W>(key[k], a.table, a.table_mask, a.table_bmask, &st->error);
       if (sm.rec_on) {
         a.rec_idx[sm.rec_base + r] = REC_NONE;
         store_key<W>(a.rec_keys + sm.rec_key_base * W, r, key[k]);
@@ -1636,11 +1646,11 @@ __global__ void grad_reduce_kernel(const double* grad_part, int grid, const long
 }
 
 template <int W>
-__global__ void rebuild_kernel(const u64* keys, u64 N, u64* table, u64 mask, u32* error) {
+__global__ void rebuild_kernel(const u64* keys, u64 N, u64* table, u64 mask, u64 bmask, u32* error) {
   for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (u64)gridDim.x * blockDim.x) {
     u64 key[W];
     load_key<W>(keys, r, key);
-    insert<W>(key, r, table, mask, error);
+    insert<W>(key, r, table, mask, bmask, error);
   }
 }
 
@@ -1749,10 +1759,10 @@ cudaError_t launch_expect(const ExpectArgs& a, const u64* keys, const double* co
 }
 
 template <int W>
-cudaError_t launch_rebuild(const u64* keys, u64 n, u64* table, u64 mask, u32* error, cudaStream_t s) {
+cudaError_t launch_rebuild(const u64* keys, u64 n, u64* table, u64 mask, u64 bmask, u32* error, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   const u64 blocks = (n + 255) / 256;
-  rebuild_kernel<W><<<(int)(blocks < 8192 ? blocks : 8192), 256, 0, s>>>(keys, n, table, mask, error);
+  rebuild_kernel<W><<<(int)(blocks < 8192 ? blocks : 8192), 256, 0, s>>>(keys, n, table, mask, bmask, error);
   return cudaGetLastError();
 }
 
@@ -1782,7 +1792,7 @@ cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const
 #define PQ_INSTANTIATE_W(Wv)                                                                            \
   PQ_INSTANTIATE(Wv, 0)                                                                                 \
   PQ_INSTANTIATE(Wv, 1)                                                                                 \
-  template cudaError_t launch_rebuild<Wv>(const u64*, u64, u64*, u64, u32*, cudaStream_t);              \
+  template cudaError_t launch_rebuild<Wv>(const u64*, u64, u64*, u64, u64, u32*, cudaStream_t);         \
   template cudaError_t launch_conjugate<Wv>(const u64*, const double*, u64, const u64*, const int*, u32, int, \
                                             u64*, double*, cudaStream_t);
 

@@ -32,6 +32,7 @@ __host__ __device__ inline u32 fused_count(u32 kind) {
   return kind == OP_GATE2 ? 2u : (kind == OP_GATE3 ? 3u : (kind == OP_GATE4 ? 4u : 1u));
 }
 
+constexpr u32 GROUP_MAX = 2;    // rotations of a fused group (OP_GATE2, gate2_tiles)
 constexpr u32 CLASS_MAX = 64;   // rotations of one class op (a row's class mask is one u64)
 constexpr u32 CLASS_KMAX = 10;  // largest family dimension (class rotations one row anticommutes with)
 
@@ -94,6 +95,7 @@ struct SweepArgs {
   double* coeffs[2];
   u64* table;              // open-addressing slots: (fingerprint << 32) | row
   u64 table_mask;
+  u64 table_bmask;         // ~(slots per bucket - 1): where a key's probe starts
   u64 cap;                 // rows each buffer holds
   u64 grid_rows;           // stop before an op whose live count exceeds this, 0 = never (see grid_stop)
   u64* status;             // tile look-back status words
@@ -145,6 +147,9 @@ struct SweepArgs {
   // microseconds before its first op, so that the other blocks' bounded waits
   // on it run out.  hold_us 0 = off.
   u32 hold_block, hold_us;
+  // Rows per thread of a many-row gate tile (1-4; 0 = 4).
+  u32 tile_items;
+  u32 pad1_;
 };
 
 enum : u32 { LOG_HELD = 0, LOG_L1 = 1, LOG_MAX = 2, LOG_EMITTED = 3, LOG_HITS = 4, LOG_WORDS = 5 };
@@ -227,7 +232,8 @@ template <int W, int ALG>
 cudaError_t launch_expect(const ExpectArgs& a, const u64* keys, const double* coeffs, u64 n,
                           ExpectPartial* partials, int grid, cudaStream_t s);
 template <int W>
-cudaError_t launch_rebuild(const u64* keys, u64 n, u64* table, u64 table_mask, u32* error, cudaStream_t s);
+cudaError_t launch_rebuild(const u64* keys, u64 n, u64* table, u64 table_mask, u64 bucket_mask, u32* error,
+                           cudaStream_t s);
 template <int W>
 cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const u64* frame_images,
                              const int* frame_signs, u32 frame_rows, int alg, u64* out_keys,

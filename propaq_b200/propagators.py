@@ -253,7 +253,7 @@ class _Propagator:
 
 
 def expectation_values(jobs, blocks_per_sm: int = 0, split: int = 1, rebalance_pct: int = 25, device: int = 0,
-                       autotune: bool = False):
+                       autotune: bool = False, fuse_max: int = 0, tile_items: int = 0, bucket_slots: int = 0):
     """Expectation values of many independent propagations in shared
     persistent launches on one GPU (pq_run_batch).
 
@@ -267,9 +267,10 @@ def expectation_values(jobs, blocks_per_sm: int = 0, split: int = 1, rebalance_p
     blocks_per_sm: grid size per SM (0 = as many as fit); split: 0 shares the
     grid equally among the jobs, 1 in proportion to their remaining work;
     rebalance_pct: re-split the grid among the running jobs once this share of
-    it is idle (0 = never).  autotune: choose these three by measurement
-    instead (propaq_b200.tuning; the first batch of a shape runs once per
-    candidate setting, later ones reuse the choice).
+    it is idle (0 = never).  fuse_max, tile_items, bucket_slots: the kernel
+    knobs of pq_batch_tuning (0 = the engine's defaults).  autotune: choose all
+    six by measurement instead (propaq_b200.tuning; the first batch of a shape
+    runs once per setting tried, later ones reuse the choice).
     """
     jobs = list(jobs)
     if not jobs:
@@ -285,7 +286,9 @@ def expectation_values(jobs, blocks_per_sm: int = 0, split: int = 1, rebalance_p
 
         t = default_tuner().tune(items, device)
         blocks_per_sm, split, rebalance_pct = t.blocks_per_sm, t.split, t.rebalance_pct
-    out = eng.run_batch(items, blocks_per_sm=blocks_per_sm, split=split, rebalance_pct=rebalance_pct)
+        fuse_max, tile_items, bucket_slots = t.fuse_max, t.tile_items, t.bucket_slots
+    out = eng.run_batch(items, blocks_per_sm=blocks_per_sm, split=split, rebalance_pct=rebalance_pct,
+                        fuse_max=fuse_max, tile_items=tile_items, bucket_slots=bucket_slots)
     results = []
     for (prop, *_), (res, nt) in zip(jobs, out):
         prop.last_run = res

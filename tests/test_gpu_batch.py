@@ -143,7 +143,7 @@ def test_autotuned_batch(gpu_engine):
     # propagator-level call with autotune=True reuses the remembered choice.
     from harness import make_cfg
 
-    from propaq_b200.tuning import CANDIDATES, BatchTuner, batch_signature
+    from propaq_b200.tuning import CANDIDATES, KERNEL_DEFAULTS, KERNEL_DIMENSIONS, BatchTuner, batch_signature
 
     probs = mixed_problems()[:4]
     items, keep = [], []
@@ -154,7 +154,8 @@ def test_autotuned_batch(gpu_engine):
     tuner = BatchTuner()
     t = tuner.tune(items)
     assert (t.blocks_per_sm, t.split, t.rebalance_pct) in CANDIDATES
-    assert len(tuner.trials[batch_signature(items)]) == len(CANDIDATES)
+    n_kernel = sum(len([v for v in vals if v != KERNEL_DEFAULTS[d]]) for d, vals in KERNEL_DIMENSIONS.items())
+    assert len(tuner.trials[batch_signature(items)]) == len(CANDIDATES) + n_kernel
     for b, p in zip(run_gpu_batch(gpu_engine, probs, **t.as_dict()), probs):
         assert_same(b, run_gpu(gpu_engine, p))
     wl = workloads.kicked_ising(5, 6, 4)

@@ -5,7 +5,10 @@ from types import SimpleNamespace
 
 import numpy as np
 
-from propaq_b200.tuning import CANDIDATES, BatchTuner, Tuning, batch_signature
+from propaq_b200.tuning import CANDIDATES, KERNEL_DEFAULTS, KERNEL_DIMENSIONS, BatchTuner, Tuning, batch_signature
+
+# kernel settings tried after the launch candidates: every value but the default
+N_KERNEL = sum(len([v for v in vals if v != KERNEL_DEFAULTS[d]]) for d, vals in KERNEL_DIMENSIONS.items())
 
 
 def item(n_units, n_gates, max_weight=10, angle=0.3):
@@ -27,14 +30,38 @@ def test_picks_the_fastest_candidate_and_remembers_it_per_shape():
     tuner = BatchTuner()
     batch = [item(40, 100), item(90, 300)]
     assert tuner.tune(batch, run=run) == Tuning(0, 1, 50)
-    assert len(calls) == len(CANDIDATES)
+    assert len(calls) == len(CANDIDATES) + N_KERNEL
     # the same shape with other angles: remembered, no new runs
     again = [item(40, 100, angle=0.9), item(90, 300, angle=0.1)]
     assert tuner.tune(again, run=run) == Tuning(0, 1, 50)
-    assert len(calls) == len(CANDIDATES)
+    assert len(calls) == len(CANDIDATES) + N_KERNEL
     assert tuner.choice(again) == Tuning(0, 1, 50)
     # another shape is tuned on its own
     other = [item(40, 100, max_weight=8)]
     assert batch_signature(other) != batch_signature(batch)
     tuner.tune(other, run=run)
-    assert len(calls) == 2 * len(CANDIDATES)
+    assert len(calls) == 2 * (len(CANDIDATES) + N_KERNEL)
+
+
+def test_kernel_knobs_one_at_a_time_from_the_best_launch_setting():
+    # fuse_max 1 and bucket_slots 8 each help on their own; tile_items never
+    # does: the tuner keeps the first two, each found from the best so far
+    def run(items, t):
+        ms = 20.0 if (t.blocks_per_sm, t.split, t.rebalance_pct) == (2, 1, 25) else 30.0
+        if t.fuse_max == 1:
+            ms -= 4.0
+        if t.bucket_slots == 8:
+            ms -= 1.0
+        if t.tile_items in (1, 2):
+            ms += 2.0
+        return ms
+
+    tuner = BatchTuner()
+    batch = [item(60, 200)]
+    best = tuner.tune(batch, run=run)
+    assert best == Tuning(2, 1, 25, fuse_max=1, tile_items=0, bucket_slots=8)
+    trials = tuner.trials[batch_signature(batch)]
+    assert len(trials) == len(CANDIDATES) + N_KERNEL
+    assert min(ms for _, ms in trials) == 15.0
+    # a default value spelled out is the same setting, not measured again
+    assert len({t.resolved() for t, _ in trials}) == len(trials)
