@@ -65,9 +65,10 @@ struct Grp {
   u32 bid, nblk;
 };
 
-// Grid barrier (sense by generation), two-level: each block arrives on one of
-// BAR_GROUPS counters (each on its own 128-byte line), the last arrival of a
-// group arrives on the top counter, and the last top arrival releases
+// Grid barrier (sense by generation).  Above BAR_FLAT blocks it is two-level:
+// each block arrives on one of BAR_GROUPS counters (each on its own 128-byte
+// line), the last arrival of a group arrives on the top counter; smaller grids
+// arrive on the top counter directly.  The last top arrival releases
 // everyone by bumping the generation.  Every wait is bounded; once one
 // expires, ERR_BARRIER_TIMEOUT makes every later barrier fall through.
 // The three steps run on thread 0 of each block, after the block's
