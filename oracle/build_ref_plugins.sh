@@ -5,8 +5,10 @@
 # (examples/plugins/notebooks/02_rust_plugins.ipynb).  These plugins are test
 # fixtures for the plugin ABI; nothing in the product links them.
 set -e
-REF=${PROPAQ_REFERENCE:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+# The reference tree: PROPAQ_REFERENCE, else a directory named `reference`
+# beside the repository.
+REF=${PROPAQ_REFERENCE:-$HERE/../../reference}
 OUT="$HERE/_ref"
 # Without the reference tree (the GPU box has only the prebuilt fixtures)
 # there is nothing to build: --if-present makes that a quiet no-op.

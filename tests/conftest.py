@@ -7,8 +7,9 @@ import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 # The reference's source tree, read only by CPU tests that load its pure-Python
-# modules or stub files; they skip when it is absent (as on a GPU box).
-REFERENCE_TREE = Path(os.environ.get("PROPAQ_REFERENCE", "/root/reference"))
+# modules or stub files; they skip when it is absent (as on a GPU box).  It is
+# PROPAQ_REFERENCE, else a directory named `reference` beside the repository.
+REFERENCE_TREE = Path(os.environ.get("PROPAQ_REFERENCE") or ROOT.parent / "reference")
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(Path(__file__).resolve().parent))
 
