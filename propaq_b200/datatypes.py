@@ -64,7 +64,7 @@ def _popcount(x: int) -> int:
 class PauliString:
     """A Pauli string on n_qubits qubits, as x and z bitmasks (bit q = qubit q)."""
 
-    __slots__ = ("_x", "_z", "_n", "_key")
+    __slots__ = ("_x", "_z", "_n", "_key", "_kb")
 
     def __init__(self, x, z, n_qubits: int):
         self._x = int(x)
@@ -73,6 +73,7 @@ class PauliString:
         if self._x >> self._n or self._z >> self._n:
             raise ValueError("PauliString bitmask has bits beyond n_qubits")
         self._key = None
+        self._kb = None
 
     @property
     def n_qubits(self) -> int:
@@ -95,6 +96,14 @@ class PauliString:
         if self._key is None:
             self._key = _spread(self._x) | (_spread(self._z) << 1)
         return self._key
+
+    def key_bytes(self, n_words: int) -> bytes:
+        """The key as n_words little-endian u64 words (kept: a circuit's
+        generators are converted once, however many propagations use them)."""
+        kb = self._kb
+        if kb is None or len(kb) != 8 * n_words:
+            kb = self._kb = self.key().to_bytes(8 * n_words, "little")
+        return kb
 
     @classmethod
     def from_key(cls, key: int, n_qubits: int) -> "PauliString":

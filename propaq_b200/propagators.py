@@ -102,9 +102,19 @@ def heisenberg_gates(circuit, n_words: int, key_of):
     for layer in reversed(list(circuit.layers)):
         rots.extend(layer[::-1] if isinstance(layer, (list, tuple)) else list(layer)[::-1])
         offsets.append(len(rots))
-    keys = [key_of(r.generator) for r in rots]
     angles = np.fromiter((r.angle for r in rots), dtype=np.float64, count=len(rots))
-    return keys_to_words(keys, n_words), angles, np.array(offsets, dtype=np.uint32)
+    gens = [r.generator for r in rots]
+    if key_of is _plain_key and n_words > 1 and all(type(g) is PauliString for g in gens):
+        # keys the generators keep as bytes: one join instead of a conversion per gate
+        buf = b"".join([g.key_bytes(n_words) for g in gens])
+        words = np.frombuffer(buf, dtype="<u8").reshape(len(gens), n_words).astype(np.uint64)
+    else:
+        words = keys_to_words([key_of(g) for g in gens], n_words)
+    return words, angles, np.array(offsets, dtype=np.uint32)
+
+
+def _plain_key(term) -> int:
+    return term.key()
 
 
 def keys_to_words(keys, n_words: int) -> np.ndarray:
@@ -201,7 +211,8 @@ class _Propagator:
         rc.want_terms = 1 if want_terms else 0
         rc.log_gates = 1 if self.logger is not None else 0
         obs_keys, obs_coeffs = observable.to_arrays(n_words)
-        gw, ga, off = heisenberg_gates(circuit, n_words, self._key)
+        gw, ga, off = heisenberg_gates(circuit, n_words,
+                                       _plain_key if type(self)._key is _Propagator._key else self._key)
         diag = None if initial_state is None else state_words(initial_state, n_units)
         args = (rc, obs_keys, obs_coeffs, gw, ga, off, diag)
         return args, n_words, n_units, (tables, plugin, cfg)

@@ -111,6 +111,26 @@ def test_heisenberg_order():
     assert list(off) == [0, 1, 3]
 
 
+def test_gate_words_from_cached_key_bytes():
+    # the propagators' path (keys kept as bytes on the generators) gives the
+    # same words as converting every key, at every width, and again after the
+    # generators were used at another width
+    from propaq_b200.propagators import _plain_key
+
+    rng = np.random.default_rng(3)
+    for n, n_words in [(100, 4), (200, 8), (60, 2), (100, 4)]:
+        layers = [[pq.PauliRotation(PauliString(int(rng.integers(0, 1 << 60)) << (n - 60),
+                                                int(rng.integers(0, 1 << 60)), n), float(rng.normal()))
+                   for _ in range(5)] for _ in range(4)]
+        circ = pq.PauliCircuit(layers)
+        fast = heisenberg_gates(circ, n_words, _plain_key)
+        slow = heisenberg_gates(circ, n_words, lambda g: g.key())
+        for f, s in zip(fast, slow):
+            assert f.dtype == s.dtype and np.array_equal(f, s)
+        wider = heisenberg_gates(circ, 2 * n_words, _plain_key)[0]
+        assert np.array_equal(wider[:, :n_words], slow[0]) and not wider[:, n_words:].any()
+
+
 def _keys_of(p):
     return np.array([p.key()], dtype=np.uint64)
 
