@@ -111,6 +111,37 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def random_sector_rate(device, gib: int = 4, n: int = 1 << 26, reps: int = 5) -> dict:
+    """The rate at which this GPU serves scattered reads from memory far larger
+    than L2: n 8-byte elements gathered from random positions of a `gib` GiB
+    buffer (torch.index_select), each landing in a 32-byte sector of its own.
+    A reference point for the HBM-bound sweep, whose partner lookups are such
+    reads: `sector_gbs` counts 32 bytes per gathered element, `dram_gbs` adds
+    the index and result streams (8 + 8 bytes per element)."""
+    import torch
+
+    x = torch.ones(gib * (1 << 30) // 8, dtype=torch.float64, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(7)
+    idx = torch.randint(0, x.numel(), (n,), device=device, dtype=torch.int64, generator=gen)
+    out = torch.empty(n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.index_select(x, 0, idx, out=out)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    for _ in range(reps):
+        torch.index_select(x, 0, idx, out=out)
+    e.record()
+    torch.cuda.synchronize()
+    sec = s.elapsed_time(e) / 1e3 / reps
+    rate = {"elements_per_s": n / sec, "sector_gbs": n * 32 / sec / 1e9, "dram_gbs": n * 48 / sec / 1e9,
+            "how": f"{n} random 8-byte reads from a {gib} GiB buffer, torch.index_select, {reps} reps"}
+    del x, idx, out
+    torch.cuda.empty_cache()
+    return rate
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle samples during the timed region."""
 
@@ -757,6 +788,13 @@ def main():
         per_step = json.loads(tf.read_text()).get("dram_bytes_per_step")
         if per_step is not None:
             traffic = per_step / (sweep_launches / args.steps)
+    # For the HBM-bound Majorana runs: the sweep's DRAM rate (traffic over the
+    # launch time) beside the rate random 32-byte reads reach on this GPU.
+    scattered = None
+    if wl.basis == 1 and traffic is not None and sweep_ms > 0:
+        rate = random_sector_rate(f"cuda:{local}")
+        dram_gbs = traffic / (sweep_ms / max(1, sweep_launches) / 1e3) / 1e9
+        scattered = dict(rate, sweep_dram_gbs=dram_gbs, sweep_frac_of_scattered=dram_gbs / rate["dram_gbs"])
     line = dict(base_line, value=value, ms_per_step=1e3 * dev_s / args.steps,
                 e2e={"value": e2e_value, "unit": "terms/s", "h2d_bytes_per_step": int(h2d),
                      "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s / args.steps},
@@ -769,7 +807,8 @@ def main():
                           "ms_per_launch": sweep_ms / max(1, sweep_launches),
                           "share_of_device_time": sweep_ms / dev_ms if dev_ms else None,
                           "gate_ops_gbs": galg / (gate_ms / 1e3) / 1e9 if gate_ms > 0 else None,
-                          "us_per_gate_op": 1e3 * gate_ms / max(1, gate_ops)},
+                          "us_per_gate_op": 1e3 * gate_ms / max(1, gate_ops),
+                          "scattered_reads": scattered},
                 clocks=clocks, peak_terms=peak, expectation_value=r.expectation_value)
     line["config"]["parallelism"] = f"replicas x{world}"
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
