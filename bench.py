@@ -62,8 +62,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="sweep blocks per SM (0 = by live count; batch: as many as fit)")
-    ap.add_argument("--fuse-max", type=int, default=0, help="rotations fused into one pass, 1-4 (0 = the engine's 4)")
+    ap.add_argument("--fuse-max", type=int, default=0, help="rotations fused into one pass, 1-2 (0 = the engine's 2)")
     ap.add_argument("--tile-items", type=int, default=0, help="rows per thread of a many-row gate tile, 1-4 (0 = 4)")
+    ap.add_argument("--no-scattered-reference", action="store_true",
+                    help="Majorana lines: skip the scattered-read reference rate (5 GB of device memory)")
     ap.add_argument("--bucket-slots", type=int, default=0, help="hash-table bucket width: 2, 4 or 8 (0 = 4)")
     ap.add_argument("--split", type=int, default=1, help="batch: 0 equal grid shares, 1 by remaining work")
     ap.add_argument("--rebalance-pct", type=int, default=25, help="batch: re-split when this %% of the grid idles")
@@ -791,7 +793,7 @@ def main():
     # For the HBM-bound Majorana runs: the sweep's DRAM rate (traffic over the
     # launch time) beside the rate random 32-byte reads reach on this GPU.
     scattered = None
-    if wl.basis == 1 and traffic is not None and sweep_ms > 0:
+    if wl.basis == 1 and traffic is not None and sweep_ms > 0 and not args.no_scattered_reference:
         rate = random_sector_rate(f"cuda:{local}")
         dram_gbs = traffic / (sweep_ms / max(1, sweep_launches) / 1e3) / 1e9
         scattered = dict(rate, sweep_dram_gbs=dram_gbs, sweep_frac_of_scattered=dram_gbs / rate["dram_gbs"])
