@@ -68,13 +68,24 @@ __device__ __forceinline__ void member_key(const u64* rep, const GateDesc<W>* cg
 
 __device__ __forceinline__ bool key_bit(const u64* k, u32 bit) { return (k[bit >> 6] >> (bit & 63)) & 1ull; }
 
-// The class rotations a key anticommutes with (bit j = rotation j).
+// The class rotations a key anticommutes with (bit j = rotation j).  For
+// Pauli keys from `fold`, the class's pair-swapped generators (W words each)
+// in shared memory: the one part of the descriptors every row reads.
 template <int W, int ALG>
-__device__ __forceinline__ u64 class_mask(const u64* key, const GateDesc<W>* cg, u32 m) {
-  using Ops = typename Alg<ALG>::T;
+__device__ __forceinline__ u64 class_mask(const u64* key, const GateDesc<W>* cg, const u64* fold, u32 m) {
   u64 s = 0;
-  for (u32 j = 0; j < m; ++j)
-    if (Ops::template anticommutes<W>(cg[j].g, key)) s |= 1ull << j;
+  if constexpr (ALG == 0) {
+    for (u32 j = 0; j < m; ++j) {
+      u64 acc = 0;
+#pragma unroll
+      for (int w = 0; w < W; ++w) acc ^= key[w] & fold[j * W + w];
+      if (popc(acc) & 1) s |= 1ull << j;
+    }
+  } else {
+    using Ops = typename Alg<ALG>::T;
+    for (u32 j = 0; j < m; ++j)
+      if (Ops::template anticommutes<W>(cg[j].g, key)) s |= 1ull << j;
+  }
   return s;
 }
 
@@ -349,13 +360,13 @@ __device__ __forceinline__ u32 block_excl_scan(u32 v, ClassSmem& cs) {
 
 // Phase A for the rows of this block: class masks and family membership.
 template <int W, int ALG>
-__device__ __noinline__ void class_phase_a(const SweepArgs& a, const GateDesc<W>* cg, u32 m, u32 op, u64 N,
-                                           const u64* keys, const Grp grp) {
+__device__ __noinline__ void class_phase_a(const SweepArgs& a, const GateDesc<W>* cg, const u64* fold, u32 m, u32 op,
+                                           u64 N, const u64* keys, const Grp grp) {
   SweepState* st = a.st;
   for (u64 r = (u64)grp.bid * BLOCK + threadIdx.x; r < N; r += (u64)grp.nblk * BLOCK) {
     u64 key[W];
     load_key<W>(keys, r, key);
-    const u64 S = class_mask<W, ALG>(key, cg, m);
+    const u64 S = class_mask<W, ALG>(key, cg, fold, m);
     a.cls_mask[r] = S;
     if (!S) continue;
     u64 rep[W];
@@ -498,21 +509,22 @@ __device__ __noinline__ u32 class_tile(const SweepArgs& a, const ClassRules<W, A
 template <int W, int ALG>
 __device__ __noinline__ int class_op(const SweepArgs& a, const GateDesc<W>* gd, u32 m, u32 op, u64 N, u64* keys,
                                      double* coeffs, TileSmem& sm, const Grp grp, u64* n_out, u32& gen) {
-  __shared__ GateDesc<W> cg[CLASS_MAX];
+  // The class's rotations are read where the host put them (through L1),
+  // except the pair-swapped generators every row's class mask reads: a shared
+  // copy of up to 64 whole descriptors took 6-12 KB of every block's L1 for
+  // all ops of every sweep, class or not (the gradient's forward runs, which
+  // form no class, went 67.7 -> 72.1 ms).
+  const GateDesc<W>* cg = gd;
+  __shared__ u64 fold[ALG == 0 ? CLASS_MAX * W : 1];
   __shared__ ClassSmem cs;
   SweepState* st = a.st;
-  {  // the class's rotations into shared memory, word by word
-    constexpr int WPD = sizeof(GateDesc<W>) / 8;
-    const u64* src = reinterpret_cast<const u64*>(gd);
-    u64* dst = reinterpret_cast<u64*>(cg);
-    for (u32 i = threadIdx.x; i < m * WPD; i += BLOCK) dst[i] = __ldg(src + i);
-    for (u32 j = threadIdx.x; j < CLASS_MAX; j += BLOCK) {
-      cs.children[j] = 0;
-      cs.anti[j] = 0;
-    }
+  for (u32 i = threadIdx.x; i < m * W; i += BLOCK) fold[i] = __ldg(&gd[i / W].g.fold[i % W]);
+  for (u32 j = threadIdx.x; j < CLASS_MAX; j += BLOCK) {
+    cs.children[j] = 0;
+    cs.anti[j] = 0;
   }
   __syncthreads();
-  class_phase_a<W, ALG>(a, cg, m, op, N, keys, grp);
+  class_phase_a<W, ALG>(a, cg, fold, m, op, N, keys, grp);
   grid_barrier(st, gen, grp);
   if (*(volatile u32*)&st->error) return 1;  // the host re-clears the family table after a failed run
   ClassRules<W, ALG> R;
