@@ -1669,6 +1669,12 @@ __global__ void conjugate_kernel(const u64* keys, const double* coeffs, u64 n, c
 
 }  // namespace
 
+// Blocks of `k` that fit on every SM at once (the grid of a cooperative
+// launch).  Once per kernel it also asks for the smallest shared-memory share
+// of the SM's unified L1 / shared memory that keeps that many blocks
+// resident: the sweeps are chains of dependent loads, and the rest of the
+// 256 KB is L1 for their rows, descriptors and local memory.  If the smaller
+// share would cost a resident block, the driver's default stays.
 template <class Kernel>
 int co_resident_grid(Kernel k, int blocks_per_sm, int* sms, int* per_sm) {
   if (!*sms) {
@@ -1677,6 +1683,20 @@ int co_resident_grid(Kernel k, int blocks_per_sm, int* sms, int* per_sm) {
     cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev);
     int p = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, k, BLOCK, 0);
+    int smem_sm = 0, reserved = 0;
+    cudaFuncAttributes fa{};
+    if (p > 0 && cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess &&
+        cudaFuncGetAttributes(&fa, k) == cudaSuccess && smem_sm > 0) {
+      const size_t need = (size_t)p * (fa.sharedSizeBytes + (size_t)reserved);
+      const int pct = (int)((need * 100 + (size_t)smem_sm - 1) / (size_t)smem_sm);
+      if (pct < 100 && cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct) == cudaSuccess) {
+        int p2 = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p2, k, BLOCK, 0);
+        if (p2 < p) cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, -1);
+      }
+      cudaGetLastError();  // a refused hint is not an error of the run
+    }
     *per_sm = p < 1 ? 1 : p;
   }
   const int b = (blocks_per_sm > 0 && blocks_per_sm < *per_sm) ? blocks_per_sm : *per_sm;
