@@ -1130,25 +1130,27 @@ int absorb_state(pq_engine* E, Slot& S, Plan& P, const pq::SweepState& h) {
 // needs them: 35 ms at the largest grid, 76 ms at one block per SM).
 struct GridChoice {
   int grid;
-  u64 rows;  // 0: no limit
-  bool occ;  // launch sweep_kernel_occ
+  u64 rows;   // 0: no limit
+  int build;  // pq::SweepBuild of the kernel to launch
 };
 constexpr u64 OCC_ROWS = 1ULL << 24;
 GridChoice choose_grid(const Plan& P, const Inputs& in, int max_grid) {
-  if (in.cfg->blocks_per_sm != 0) return {max_grid, 0, false};
-  const auto tier = [&](int bps, bool occ) {
+  if (in.cfg->blocks_per_sm != 0) return {max_grid, 0, pq::SWEEP_DEFAULT};
+  const auto tier = [&](int bps, int build) {
     return with_words(P.W, [&](auto w) {
       constexpr int WW = decltype(w)::value;
-      return P.alg == 0 ? pq::sweep_grid<WW, 0>(bps, occ) : pq::sweep_grid<WW, 1>(bps, occ);
+      return P.alg == 0 ? pq::sweep_grid<WW, 0>(bps, build) : pq::sweep_grid<WW, 1>(bps, build);
     });
   };
-  const int g1 = tier(1, false), g2 = tier(2, false);
+  // the one- and two-block tiers run the two-block build (keys of at most 4 words)
+  const int small = P.W <= 4 ? pq::SWEEP_TWO : pq::SWEEP_DEFAULT;
+  const int g1 = tier(1, small), g2 = tier(2, small);
   const u64 r1 = (u64)g1 * 256, r2 = 1ULL << 20;
-  if (g1 < max_grid && P.n_live <= r1) return {g1, r1, false};
-  if (g2 < max_grid && P.n_live <= r2) return {g2, r2, false};
-  if (P.W > 2) return {max_grid, 0, false};
-  if (P.n_live <= OCC_ROWS) return {max_grid, OCC_ROWS, false};
-  return {tier(0, true), 0, true};
+  if (g1 < max_grid && P.n_live <= r1) return {g1, r1, small};
+  if (g2 < max_grid && P.n_live <= r2) return {g2, r2, small};
+  if (P.W > 2) return {max_grid, 0, pq::SWEEP_DEFAULT};
+  if (P.n_live <= OCC_ROWS) return {max_grid, OCC_ROWS, pq::SWEEP_DEFAULT};
+  return {tier(0, pq::SWEEP_SIX), 0, pq::SWEEP_SIX};
 }
 
 // Runs every built op of one plan, relaunching after capacity growth and when
@@ -1177,8 +1179,8 @@ int execute_launches(pq_engine* E, Slot& S, Plan& P, int grid, bool* began, size
     cudaEventRecord(E->ev_l0, E->stream);
     e = with_words(P.W, [&](auto w) {
       constexpr int WW = decltype(w)::value;
-      return P.alg == 0 ? pq::launch_sweep<WW, 0>(a, grid, E->stream, gc.occ)
-                        : pq::launch_sweep<WW, 1>(a, grid, E->stream, gc.occ);
+      return P.alg == 0 ? pq::launch_sweep<WW, 0>(a, grid, E->stream, gc.build)
+                        : pq::launch_sweep<WW, 1>(a, grid, E->stream, gc.build);
     });
     if (e != cudaSuccess) return E->cuda_fail(e, "sweep launch");
     cudaEventRecord(E->ev_l1, E->stream);

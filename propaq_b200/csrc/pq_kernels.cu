@@ -1340,6 +1340,15 @@ __global__ void __launch_bounds__(BLOCK, 6) sweep_kernel_occ(const SweepArgs a) 
   sweep_body<W, ALG>(a, Grp{blockIdx.x, gridDim.x});
 }
 
+// The same sweep for keys of at most 4 words, compiled for two resident
+// blocks of 256 per SM (up to 128 registers a thread, no spills in the op
+// paths): the grids of one and two blocks per SM that small and mid-size live
+// sets run on.
+template <int W, int ALG>
+__global__ void __launch_bounds__(BLOCK, 2) sweep_kernel_two(const SweepArgs a) {
+  sweep_body<W, ALG>(a, Grp{blockIdx.x, gridDim.x});
+}
+
 // A batch: each instance owns the contiguous blocks [blk_begin, blk_begin +
 // blk_count) of the cooperative grid and runs its own op sequence with its own
 // barrier; block_inst maps a block to its instance.  Instances run at WM or
@@ -1704,11 +1713,17 @@ int co_resident_grid(Kernel k, int blocks_per_sm, int* sms, int* per_sm) {
 }
 
 template <int W, int ALG>
-int sweep_grid(int blocks_per_sm, bool occ) {
+int sweep_grid(int blocks_per_sm, int build) {
   if constexpr (W <= 2) {
-    if (occ) {
+    if (build == SWEEP_SIX) {
       static int sms = 0, per_sm = 0;
       return co_resident_grid(sweep_kernel_occ<W, ALG>, blocks_per_sm, &sms, &per_sm);
+    }
+  }
+  if constexpr (W <= 4) {
+    if (build == SWEEP_TWO) {
+      static int sms = 0, per_sm = 0;
+      return co_resident_grid(sweep_kernel_two<W, ALG>, blocks_per_sm, &sms, &per_sm);
     }
   }
   static int sms = 0, per_sm = 0;
@@ -1722,12 +1737,15 @@ int batch_grid(int blocks_per_sm) {
 }
 
 template <int W, int ALG>
-cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s, bool occ) {
+cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s, int build) {
   SweepArgs args = a;
   void* params[] = {&args};
   const void* k = (const void*)sweep_kernel<W, ALG>;
   if constexpr (W <= 2) {
-    if (occ) k = (const void*)sweep_kernel_occ<W, ALG>;
+    if (build == SWEEP_SIX) k = (const void*)sweep_kernel_occ<W, ALG>;
+  }
+  if constexpr (W <= 4) {
+    if (build == SWEEP_TWO) k = (const void*)sweep_kernel_two<W, ALG>;
   }
   return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(BLOCK), params, 0, s);
 }
@@ -1801,9 +1819,9 @@ cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const
 }
 
 #define PQ_INSTANTIATE(Wv, Av)                                                                          \
-  template int sweep_grid<Wv, Av>(int, bool);                                                              \
+  template int sweep_grid<Wv, Av>(int, int);                                                              \
   template int batch_grid<Wv, Av>(int);                                                                    \
-  template cudaError_t launch_sweep<Wv, Av>(const SweepArgs&, int, cudaStream_t, bool);                 \
+  template cudaError_t launch_sweep<Wv, Av>(const SweepArgs&, int, cudaStream_t, int);                 \
   template cudaError_t launch_batch_sweep<Wv, Av>(const SweepArgs*, const u32*, int, cudaStream_t);     \
   template cudaError_t launch_adjoint<Wv, Av>(const AdjointArgs&, int, cudaStream_t);                   \
   template cudaError_t launch_adjoint_seed<Wv, Av>(const ExpectArgs&, const u64*, u64, double*, cudaStream_t); \

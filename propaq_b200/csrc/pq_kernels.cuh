@@ -198,15 +198,19 @@ struct ExpectPartial {
   u64 below;        // |c| < min_coeff
 };
 
-// Co-resident grid of the sweep kernel for this W / algebra: every SM with
-// blocks_per_sm blocks (0 or more than fit = as many as fit).  occ selects,
-// for 1- and 2-word keys, the build of the sweep for six resident blocks per
-// SM (for live sets of 2^24 rows and more); wider keys ignore it.
+// Builds of the sweep kernel: for its default occupancy (MinBlocks), for six
+// resident blocks per SM (1- and 2-word keys, live sets of 2^24 rows and
+// more), for two (keys of at most 4 words, the one- and two-block-per-SM
+// grids).  A width without the build asked for takes the default one.
+enum SweepBuild : int { SWEEP_DEFAULT = 0, SWEEP_SIX = 1, SWEEP_TWO = 2 };
+
+// Co-resident grid of the sweep kernel for this W / algebra and build: every
+// SM with blocks_per_sm blocks (0 or more than fit = as many as fit).
 template <int W, int ALG>
-int sweep_grid(int blocks_per_sm, bool occ = false);
+int sweep_grid(int blocks_per_sm, int build = SWEEP_DEFAULT);
 
 template <int W, int ALG>
-cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s, bool occ = false);
+cudaError_t launch_sweep(const SweepArgs& a, int grid, cudaStream_t s, int build = SWEEP_DEFAULT);
 // Batched sweep of instances with keys WM or WM / 2 words wide (n_words):
 // args[i] describes instance i and its blk_begin / blk_count slice of the
 // grid; block_inst[b] is the instance of block b.  batch_grid is its
