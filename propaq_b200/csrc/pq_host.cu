@@ -1509,14 +1509,14 @@ int finish(pq_engine* E, Slot& S, Plan& P, const std::vector<pq::ExpectPartial>&
             std::memcpy(&rcd.discarded_coeff_max, &w[pq::LOG_MAX], 8);
           }
           // the op's device time; a fused op's time goes to its first rotation
-          rcd.elapsed_ms = op > 0 ? (double)(stamps[op] - stamps[op - 1]) * 1e-6 : 0.0;
+          rcd.elapsed_ms = op > 0 && stamps[op] > stamps[op - 1] ? (double)(stamps[op] - stamps[op - 1]) * 1e-6 : 0.0;
         }
       }
   }
   for (size_t i = 0; i < no; ++i) {
     if (pq::is_class(P.ops[i].kind)) ++res->class_ops;
     const u64 n_in = i ? hist[i - 1] : P.n0;
-    const double op_ms = i ? (double)(stamps[i] - stamps[i - 1]) * 1e-6 : 0.0;
+    const double op_ms = i && stamps[i] > stamps[i - 1] ? (double)(stamps[i] - stamps[i - 1]) * 1e-6 : 0.0;
     switch (pq::is_class(P.ops[i].kind) ? (u32)pq::OP_GATE : P.ops[i].kind) {
       case pq::OP_GATE:
       case pq::OP_GATE2:

@@ -1226,7 +1226,14 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Grp grp) {
           if (i + 1 < nops) {
             grid_barrier(st, gen, grp);
             Ni = ld_volatile(out_i);
-            if (grp.bid == 0 && threadIdx.x == 0) a.hist[op + i] = Ni;
+            if (grp.bid == 0 && threadIdx.x == 0) {
+              a.hist[op + i] = Ni;
+              if (a.stamps) {  // a capacity stop before the next rotation leaves no other stamp for this one
+                u64 t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                a.stamps[op + i] = t;
+              }
+            }
           }
         }
         if (stopped) break;

@@ -439,3 +439,20 @@ def test_propagate_returns_oracle_terms(gpu_engine, oracle):
     o = run_oracle(oracle, from_workload(wl))
     want = {PauliString.from_key(int(k[0]), 10): c for k, c in zip(o.keys, o.coeffs)}
     assert dict(out.items()) == want
+
+
+def test_op_times_on_a_fresh_engine():
+    # A fresh engine grows its buffers inside fused pairs (a capacity stop
+    # between the two rotations): every op still has its device time, so the
+    # per-kind sums stay finite and no gate record is negative or huge.
+    from propaq_b200 import _native as nat
+
+    p = from_workload(workloads.kicked_ising(8, 8, 6))
+    eng = nat.Engine(0)
+    for _ in range(2):
+        cfg, keep = make_cfg(p, want_terms=False)
+        res, nt = eng.run(cfg, p.obs_keys, p.obs_coeffs, p.gate_keys, p.angles, p.offsets, p.diag)
+        assert int(res.sweep_launches) >= 1
+        total = res.gate_ms + res.noise_ms + res.phase_ms
+        assert 0.0 < total < 1e4, (res.gate_ms, res.noise_ms, res.phase_ms)
+        assert res.gate_ms <= 10.0 * res.device_ms + 10.0
