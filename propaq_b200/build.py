@@ -20,10 +20,13 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libpropaq_cuda.so"
-# The 16-, 32- and 64-word kernels are separate translation units (they
-# include pq_kernels.cu) so that they compile in parallel with the rest.
-SOURCES = ["pq_kernels_w64.cu", "pq_kernels_w32.cu", "pq_kernels_w16.cu", "pq_kernels.cu", "pq_host.cu",
-           "pq_noalloc.cu", "pq_sort.cu"]
+# The 4-, 8-, 16-, 32- and 64-word kernels are separate translation units
+# (they include pq_kernels.cu; the 32- and 64-word ones split again by
+# algebra) so that they compile in parallel with the rest; the longest
+# compiles come first.
+WIDTH_UNITS = ["pq_kernels_w64.cu", "pq_kernels_w64_majorana.cu", "pq_kernels_w32.cu", "pq_kernels_w32_majorana.cu",
+               "pq_kernels_w16.cu", "pq_kernels_w4.cu", "pq_kernels_w8.cu"]
+SOURCES = WIDTH_UNITS[:4] + ["pq_kernels.cu"] + WIDTH_UNITS[4:] + ["pq_host.cu", "pq_noalloc.cu", "pq_sort.cu"]
 HEADERS = ["pq_device.cuh", "pq_kernels.cuh", "pq_tableau.h", "pq_class.cuh", "pq_sort.cuh"]
 
 NVCC_FLAGS = [
@@ -61,9 +64,7 @@ def _obj(src: str) -> Path:
 _KERNEL_DEPS = ["pq_device.cuh", "pq_kernels.cuh", "pq_class.cuh"]
 DEPS = {
     "pq_kernels.cu": _KERNEL_DEPS,
-    "pq_kernels_w16.cu": _KERNEL_DEPS + ["pq_kernels.cu"],
-    "pq_kernels_w32.cu": _KERNEL_DEPS + ["pq_kernels.cu"],
-    "pq_kernels_w64.cu": _KERNEL_DEPS + ["pq_kernels.cu"],
+    **{u: _KERNEL_DEPS + ["pq_kernels.cu"] for u in WIDTH_UNITS},
     "pq_host.cu": ["pq_device.cuh", "pq_kernels.cuh", "pq_sort.cuh", "pq_tableau.h", "../../include/propaq_cuda.h"],
     "pq_noalloc.cu": ["pq_device.cuh", "../../include/propaq_cuda.h"],
     "pq_sort.cu": ["pq_device.cuh", "pq_sort.cuh"],

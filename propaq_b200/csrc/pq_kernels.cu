@@ -1835,24 +1835,31 @@ cudaError_t launch_conjugate(const u64* keys, const double* coeffs, u64 n, const
   template int adjoint_grid<Wv, Av>();                                                                  \
   template cudaError_t launch_expect<Wv, Av>(const ExpectArgs&, const u64*, const double*, u64,         \
                                              ExpectPartial*, int, cudaStream_t);
-#define PQ_INSTANTIATE_W(Wv)                                                                            \
-  PQ_INSTANTIATE(Wv, 0)                                                                                 \
-  PQ_INSTANTIATE(Wv, 1)                                                                                 \
+#define PQ_INSTANTIATE_KEYS(Wv)                                                                         \
   template cudaError_t launch_rebuild<Wv>(const u64*, u64, u64*, u64, u64, u32*, cudaStream_t);         \
   template cudaError_t launch_conjugate<Wv>(const u64*, const double*, u64, const u64*, const int*, u32, int, \
                                             u64*, double*, cudaStream_t);
+#define PQ_INSTANTIATE_W(Wv)                                                                            \
+  PQ_INSTANTIATE(Wv, 0)                                                                                 \
+  PQ_INSTANTIATE(Wv, 1)                                                                                 \
+  PQ_INSTANTIATE_KEYS(Wv)
 
-// Key widths 1-8 words (up to 256 units) here; 16, 32 and 64 words each in a
-// translation unit of its own (pq_kernels_w16.cu ...) that defines
+// Key widths 1 and 2 words (up to 64 units) here; 4, 8, 16, 32 and 64 words
+// each in a translation unit of its own (pq_kernels_w4.cu ...) that defines
 // PQ_ONLY_WIDTH and includes this file, so that the widths compile in
-// parallel.
-#ifdef PQ_ONLY_WIDTH
+// parallel.  The 32- and 64-word kernels, the slowest to compile, are split
+// further by algebra: pq_kernels_w64.cu also defines PQ_ONLY_ALG 0 (Pauli,
+// with the algebra-free key kernels), pq_kernels_w64_majorana.cu PQ_ONLY_ALG 1.
+#if defined(PQ_ONLY_WIDTH) && defined(PQ_ONLY_ALG)
+PQ_INSTANTIATE(PQ_ONLY_WIDTH, PQ_ONLY_ALG)
+#if PQ_ONLY_ALG == 0
+PQ_INSTANTIATE_KEYS(PQ_ONLY_WIDTH)
+#endif
+#elif defined(PQ_ONLY_WIDTH)
 PQ_INSTANTIATE_W(PQ_ONLY_WIDTH)
 #else
 PQ_INSTANTIATE_W(1)
 PQ_INSTANTIATE_W(2)
-PQ_INSTANTIATE_W(4)
-PQ_INSTANTIATE_W(8)
 #endif
 
 }  // namespace pq
