@@ -238,7 +238,7 @@ __device__ __noinline__ void run_warp_family(const ClassRules<W, ALG>& R, const 
     member_key<W>(rep, cg, sidx, c, q);
     double cj = 0.0;
     u64 es = NO_SLOT;
-    const long long j = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, a.st, cj, es);
+    const long long j = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, a.st, cj, es, 0);
     if (j >= 0) {
       F.pres |= 1u << s;
       F.cf[s] = cj;

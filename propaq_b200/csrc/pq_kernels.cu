@@ -345,10 +345,13 @@ __device__ __forceinline__ long long lookup(const u64* q, u64 n_pre, const u64* 
 // one round trip less (cj receives it); on a miss, `empty` receives the empty
 // slot where the probe ended, which is the first slot an insert of q would
 // take (every slot before it on q's probe sequence is occupied, and occupied
-// slots stay occupied during an op), or NO_SLOT.
+// slots stay occupied during an op), or NO_SLOT.  The coefficient is loaded
+// only for candidate rows >= c_from (cj stays 0 below): a row that owns a
+// pair only when its partner's index is higher passes its own index + 1 and
+// saves, for every pair it does not own, a random sector it would not use.
 template <int W>
 __device__ long long lookup_from_c(const u64* q, u32 fp, u64 i, u64 n_pre, const u64* keys, const double* coeffs,
-                                   const u64* table, u64 mask, SweepState* st, double& cj, u64& empty) {
+                                   const u64* table, u64 mask, SweepState* st, double& cj, u64& empty, u64 c_from) {
   for (u64 probe = 0; probe <= mask; ++probe) {
     const u64 s = __ldcg(table + i);
     if (s == EMPTY_SLOT) {
@@ -358,7 +361,7 @@ __device__ long long lookup_from_c(const u64* q, u32 fp, u64 i, u64 n_pre, const
     const u32 row = (u32)s;
     if ((u32)(s >> 32) == fp && row < n_pre) {
       const u64* kp = keys + (u64)row * W;
-      const double c = __ldcg(coeffs + row);
+      const double c = row >= c_from ? __ldcg(coeffs + row) : 0.0;
       bool eq = true;
 #pragma unroll
       for (int w = 0; w < W; ++w) eq &= __ldcg(kp + w) == q[w];
@@ -376,7 +379,7 @@ __device__ long long lookup_from_c(const u64* q, u32 fp, u64 i, u64 n_pre, const
 template <int W>
 __device__ __forceinline__ long long lookup_c(const u64* q, u64 n_pre, const u64* keys, const double* coeffs,
                                               const u64* table, u64 mask, u64 bmask, SweepState* st, double& cj,
-                                              u64& empty) {
+                                              u64& empty, u64 c_from) {
   const u64 h = key_hash<W>(q);
   const u32 fp = (u32)(h >> 32);
   const u64 b = bucket_start(h, mask, bmask);
@@ -394,7 +397,7 @@ __device__ __forceinline__ long long lookup_c(const u64* q, u64 n_pre, const u64
     const u32 row = (u32)sl[m];
     if ((u32)(sl[m] >> 32) == fp && row < n_pre) {
       const u64* kp = keys + (u64)row * W;
-      const double c = __ldcg(coeffs + row);
+      const double c = row >= c_from ? __ldcg(coeffs + row) : 0.0;
       bool eq = true;
 #pragma unroll
       for (int w = 0; w < W; ++w) eq &= __ldcg(kp + w) == q[w];
@@ -404,7 +407,7 @@ __device__ __forceinline__ long long lookup_c(const u64* q, u64 n_pre, const u64
       }
     }
   }
-  return lookup_from_c<W>(q, fp, (b + 4) & mask, n_pre, keys, coeffs, table, mask, st, cj, empty);
+  return lookup_from_c<W>(q, fp, (b + 4) & mask, n_pre, keys, coeffs, table, mask, st, cj, empty, c_from);
 }
 
 // Slot value v for q placed from `start`, the empty slot a lookup of q in
@@ -577,7 +580,7 @@ __device__ __noinline__ void gate_tiles(const SweepArgs& a, const GateDesc<W>& d
       u64 q[W];
 #pragma unroll
       for (int w = 0; w < W; ++w) q[w] = key[k][w] ^ g.gen[w];
-      j[k] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cj[k], es[k]);
+      j[k] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cj[k], es[k], r + 1);
     }
     // The lower row of a pair owns both coefficients.
     u32 own = 0;
@@ -703,7 +706,7 @@ __device__ __noinline__ void gate_tiles_large(const SweepArgs& a, const GateDesc
       for (int w = 0; w < W; ++w) q[w] = key[w] ^ g.gen[w];
       double cj = 0.0;
       u64 es = NO_SLOT;
-      const long long j = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cj, es);
+      const long long j = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cj, es, r + 1);
       if (j >= 0 && (u64)j < r) continue;  // the lower row of the pair owns it
       const double bi = __dmul_rn(__dmul_rn(c, sn), neg_im(Ops::template product_exp<W>(g, key), g.sign));
       const int si = a.host_state ? (int)a.host_state[r] : state(c, q);
@@ -834,15 +837,15 @@ __device__ __noinline__ void gate2_tiles(const SweepArgs& a, const GateDesc<W>& 
       u64 q[W];
       if (a1) {
         member(1, q);
-        j[1] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cm[1], es[1]);
+        j[1] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cm[1], es[1], r + 1);
       }
       if (a2) {
         member(2, q);
-        j[2] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cm[2], es[2]);
+        j[2] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cm[2], es[2], r + 1);
       }
       if (a1 && a2) {
         member(3, q);
-        j[3] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cm[3], es[3]);
+        j[3] = lookup_c<W>(q, N, keys, coeffs, a.table, a.table_mask, a.table_bmask, st, cm[3], es[3], r + 1);
       }
     }
     const bool own = (a1 || a2) && (j[1] < 0 || (u64)j[1] > r) && (j[2] < 0 || (u64)j[2] > r) &&
