@@ -243,9 +243,10 @@ cudaError_t fold_sorted(const u64* keys, const double* coeffs, u64 n, u64* keys_
   count_scan_kernel<<<1, 1024, 0, s>>>(idx, n);
   fold_runs_kernel<W><<<grid_for(n, 256), 256, 0, s>>>(keys, coeffs, n, head, idx, keys_out, coeffs_out);
   *launches += 3;
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   u32 last_idx = 0, last_head = 0;
-  cudaMemcpyAsync(&last_idx, idx + n - 1, 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(&last_head, head + n - 1, 4, cudaMemcpyDeviceToHost, s);
+  if ((e = cudaMemcpyAsync(&last_idx, idx + n - 1, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(&last_head, head + n - 1, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
   *n_out = (u64)last_idx + last_head;
   return cudaGetLastError();
