@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--tile-items", type=int, default=0, help="rows per thread of a many-row gate tile, 1-4 (0 = 4)")
     ap.add_argument("--no-scattered-reference", action="store_true",
                     help="Majorana lines: skip the scattered-read reference rate (5 GB of device memory)")
-    ap.add_argument("--bucket-slots", type=int, default=0, help="hash-table bucket width: 2, 4 or 8 (0 = 4)")
+    ap.add_argument("--bucket-slots", type=int, default=0, help="hash-table bucket width: 2, 4 or 8 (0 = 2)")
     ap.add_argument("--split", type=int, default=1, help="batch: 0 equal grid shares, 1 by remaining work")
     ap.add_argument("--rebalance-pct", type=int, default=25, help="batch: re-split when this %% of the grid idles")
     ap.add_argument("--no-sequential", action="store_true", help="batch: skip the sequential pq_run comparison")

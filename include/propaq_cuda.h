@@ -96,7 +96,7 @@ typedef struct pq_run_config {
   uint32_t tile_items;       /* rows per thread of a many-row gate tile: 1-4
                                 (default 4)                                     */
   uint32_t bucket_slots;     /* hash-table slots a key's probe starts in: 2, 4
-                                or 8 (default 4)                                */
+                                or 8 (default 2)                                */
 } pq_run_config;
 
 /* crates/core/src/interface/results.rs:8-51 (PropagationResult), plus the

@@ -42,7 +42,7 @@ KERNEL_DIMENSIONS = {
     "tile_items": (1, 2, 4),
     "bucket_slots": (2, 4, 8),
 }
-KERNEL_DEFAULTS = {"fuse_max": 2, "tile_items": 4, "bucket_slots": 4}
+KERNEL_DEFAULTS = {"fuse_max": 2, "tile_items": 4, "bucket_slots": 2}
 
 
 @dataclass(frozen=True)
