@@ -65,3 +65,27 @@ def test_kernel_knobs_one_at_a_time_from_the_best_launch_setting():
     assert min(ms for _, ms in trials) == 15.0
     # a default value spelled out is the same setting, not measured again
     assert len({t.resolved() for t, _ in trials}) == len(trials)
+
+
+def test_kernel_defaults_match_the_engine():
+    # The tuner treats a knob at KERNEL_DEFAULTS as the engine's own default
+    # (0) and does not measure it twice, so the two must agree: the host's
+    # FUSE_DEFAULT and BUCKET_DEFAULT, and the kernel's MAX_ITEMS (what a
+    # tile_items of 0 runs).
+    import re
+    from pathlib import Path
+
+    csrc = Path(__file__).resolve().parent.parent / "propaq_b200" / "csrc"
+    host = (csrc / "pq_host.cu").read_text()
+    kern = (csrc / "pq_kernels.cu").read_text()
+
+    def const(text, name):
+        m = re.search(rf"constexpr\s+\w+\s+{name}\s*=\s*(\d+)\s*;", text)
+        assert m, name
+        return int(m.group(1))
+
+    assert KERNEL_DEFAULTS["fuse_max"] == const(host, "FUSE_DEFAULT")
+    assert KERNEL_DEFAULTS["bucket_slots"] == const(host, "BUCKET_DEFAULT")
+    assert KERNEL_DEFAULTS["tile_items"] == const(kern, "MAX_ITEMS")
+    for d, vals in KERNEL_DIMENSIONS.items():
+        assert KERNEL_DEFAULTS[d] in vals, d
